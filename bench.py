@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark: molecule-steps per second of the REMD hot path on one B200.
+
+Workload (default): the 256-replica uneven batch -- 8 seeded ensembles, nmol
+log-uniform in 64..2048, TIP3P/TIP4P/TIP5P, bulk / nanotube / nano-slit, rcut
+8.5..12 A (remd_b200.systems.config4) -- with interval = 100 MD steps.  One
+bench "step" is one REMD interval of the whole batch: 100 MD steps of every
+replica (integrator, forces, wall) plus the interval start/end kernels.
+
+  value      whole-job mol-steps/s with the state resident in HBM, timed with
+             CUDA events on the engine's stream (sum over the K intervals), L2
+             flushed (256 MiB write) between intervals;
+  e2e        the same metric through the public C-ABI call a user makes per
+             interval: remd_execute_steps(T, P) from host arrays (H2D of the
+             conditions, D2H of the 19 averages per replica) followed by the
+             host-side Metropolis exchange of every ensemble;
+  roofline   the force kernel (dominant): algorithmic FLOPs per launch
+             (unordered pairs within rcut x 326 for TIP3P/TIP4P, x 515 for
+             TIP5P) / its mean CUDA-event duration, against the measured FP32
+             FMA peak of this GPU;
+  cpu_baseline  the reference's own CPU code (oracle/_ref, generic FP64 build,
+             replica-parallel on all host cores) on a bounded sample.
+
+`--impl reference` times only that CPU baseline on the same workload and
+prints its line.  Multi-GPU (`--gpus N` under torchrun): every rank runs its
+own seeded copy of the workload (replicas only, no data-path collective),
+value = total mol-steps / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mol-steps/s"
+FLOP_PER_PAIR = {3: 326, 4: 326, 5: 515}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--config", type=int, default=4, choices=[1, 2, 3, 4])
+    ap.add_argument("--interval", type=int, default=100)
+    ap.add_argument("--tile", type=int, default=128)
+    ap.add_argument("--skin", type=float, default=1.0)
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
+    return ap.parse_args(argv)
+
+
+def workload(config, seed, interval):
+    from remd_b200 import systems as S
+    if config == 4:
+        return S.config4(seed=seed, interval=interval)
+    fn = {1: S.config1, 2: S.config2, 3: S.config3}[config]
+    ens = fn(seed=seed)
+    for e in ens:
+        e.spec.interval = interval
+    return ens
+
+
+def workload_desc(config, ens, interval):
+    n = [e.spec.nmol for e in ens for _ in e.states]
+    name = {4: "uneven batch: 8 ensembles / 256 replicas, TIP3P/4P/5P, bulk+tube+slit",
+            1: "TIP4P nanotube N=128, 16 replicas", 2: "TIP4P slit N=512, 64 replicas",
+            3: "TIP5P bulk N=1728, 128 replicas"}[config]
+    return {"workload": name, "config_index": config, "replicas": len(n),
+            "molecules": int(sum(n)), "nmol_range": [int(min(n)), int(max(n))],
+            "interval_steps": interval, "ensembles": len(ens),
+            "models": sorted({e.spec.moltype.name for e in ens}),
+            "l2": "flushed (256 MiB write) between timed intervals",
+            "parallelism": "replicas-only"}
+
+
+# ------------------------------------------------------------------ distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x, world):
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.3 * max(sm)]
+        return {"sm_mhz": float(np.median(load or sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": float(max(power)) if power else None}
+
+
+# ------------------------------------------------------------------ CPU baseline (reference)
+def cpu_baseline(ens, nsteps, nthreads):
+    """The reference's own CPU code (oracle/_ref generic FP64 build), every
+    replica advanced nsteps MD steps, replicas spread over nthreads host threads."""
+    from oracle import oracle as O
+    kind = "reference"
+    if not O.reference_available():
+        kind = "port"
+    refs = []
+    t0 = time.perf_counter()
+    for e in ens:
+        for st in e.states:
+            if kind == "reference":
+                r = O.Reference(e.spec, st, e.spec.moltype_file)
+                r.initialize_property()
+            else:
+                r = O.Oracle(e.spec, st)
+                r.initialize_property()
+            refs.append(r)
+    setup = time.perf_counter() - t0
+    molsteps = sum(e.spec.nmol for e in ens for _ in e.states) * nsteps
+    t0 = time.perf_counter()
+    if kind == "reference":
+        O.reference_parallel_steps(refs, nsteps, nthreads)
+        cores = nthreads
+    else:
+        for r in refs:
+            r.steps(nsteps)
+        cores = 1
+    dt = time.perf_counter() - t0
+    return {"value": molsteps / dt, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"all {len(refs)} replicas x {nsteps} MD steps "
+                      f"({'oracle/_ref generic FP64 build' if kind == 'reference' else 'C oracle'},"
+                      f" replica-parallel over {cores} threads; {dt:.1f} s timed, setup {setup:.1f} s)",
+            "seconds": dt}
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    ens = workload(args.config, args.seed, args.interval)
+    from oracle import oracle as O
+    nth = cpu_threads()
+    total = sum(e.spec.nmol for e in ens for _ in e.states)
+    # warm-up then K timed steps, each one MD step of every replica
+    b = cpu_baseline(ens, max(args.warmup, 1), nth) if args.warmup > 0 else None
+    res = cpu_baseline(ens, args.steps, nth)
+    line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["seconds"] * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_desc(args.config, ens, args.interval),
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "one step = one MD step of all replicas (bounded sample of the interval)"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ engine arm
+def profile_traffic():
+    """DRAM bytes per force launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "force_kernel_config4.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def engine_arm(args, rank, world, local):
+    import ctypes
+
+    import torch
+
+    from remd_b200 import engine as E
+    dev = local
+    torch.cuda.set_device(dev)
+    ens = workload(args.config, args.seed + 1000 * rank, args.interval)
+    eng = E.REMDGPU(ens, precision="fp32", device=dev)
+    if args.tile != 128 or args.skin != 1.0:
+        eng.set_tuning(args.tile, args.skin)
+    T = np.concatenate([e.T for e in ens])
+    P = np.concatenate([e.P for e in ens])
+    nmol_total = int(sum(e.spec.nmol for e in ens for _ in e.states))
+    mol_steps_per_interval = nmol_total * args.interval
+    stream = torch.cuda.ExternalStream(E.lib().remd_stream(eng.h))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+    for _ in range(args.warmup):
+        eng.execute_async(T, P)
+    eng.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    clocks = ClockSampler(dev)
+    barrier(world)
+    torch.cuda.synchronize()
+    eng.synchronize()
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        evs[k][0].record(stream)
+        eng.execute_async()
+        evs[k][1].record(stream)
+    eng.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    local_ms = float(sum(ms))
+    max_ms = reduce_max(local_ms, world)
+    total_units = reduce_sum(mol_steps_per_interval * args.steps, world)
+    value = total_units / (max_ms * 1e-3)
+    statuses = [eng.replica_status(r) for r in range(eng.nrep)]
+
+    # roofline of the force kernel: per-launch algorithmic FLOPs / event duration
+    eng.compute_forces()
+    flops = 0.0
+    pairs = 0
+    k = 0
+    for e in ens:
+        for _ in e.states:
+            pr = int(E.lib().remd_replica_pair_count(eng.h, k))
+            pairs += pr
+            flops += pr * FLOP_PER_PAIR[e.spec.moltype.nsite]
+            k += 1
+    prof = (ctypes.c_double * 2)()
+    E._check(E.lib().remd_profile_steps(eng.h, 10, prof))
+    force_ms, integ_ms = prof[1], prof[0]
+    peak = ctypes.c_double()
+    E._check(E.lib().remd_measure_fp32_peak(dev, ctypes.byref(peak)))
+    achieved = flops / (force_ms * 1e-3) / 1e12
+    roof = {"bound": "fp32", "kernel": "k_force (pair loop + wall + A2M)",
+            "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+            "frac": achieved / peak.value,
+            "peak_source": "measured: register-resident FP32 FMA chains on all SMs "
+                           "(remd_measure_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
+            "traffic": profile_traffic(), "pairs_per_launch": pairs,
+            "flops_per_launch": flops, "force_ms": force_ms, "integrate_ms": integ_ms}
+
+    # end to end through the public C-ABI call (host buffers, host exchange)
+    e2e = None
+    if not args.no_e2e:
+        grids = [(e.ntemp, e.npress) for e in ens]
+        idx = [np.arange(e.nreplica, dtype=np.int32) for e in ens]
+        Ts = [e.T.copy() for e in ens]
+        Ps = [e.P.copy() for e in ens]
+        rng = np.random.default_rng(123 + rank)
+        off = np.cumsum([0] + [e.nreplica for e in ens])
+        barrier(world)
+        t0 = time.perf_counter()
+        for step in range(args.steps):
+            eng.ExecuteSteps(np.concatenate(Ts), np.concatenate(Ps))
+            avg = eng.all_averages()
+            for i, e in enumerate(ens):
+                a = avg[off[i]:off[i + 1]]
+                E.exchange_host(grids[i][0], grids[i][1], e.spec.pconstant, step, idx[i], Ts[i],
+                                Ps[i], a[:, 0] + a[:, 1] + a[:, 2], a[:, 3],
+                                rng.random(max(e.nreplica // 2, 1)))
+        e2e_s = reduce_max(time.perf_counter() - t0, world)
+        e2e = {"value": total_units / e2e_s, "unit": METRIC,
+               "h2d_bytes_per_step": int(2 * 8 * eng.nrep),
+               "d2h_bytes_per_step": int(19 * 8 * eng.nrep),
+               "path": "remd_execute_steps(T,P) + remd_get_all_averages + remd_exchange_host per ensemble"}
+
+    # plain per-replica FP64 form on a sample (one replica of every ensemble)
+    plain = None
+    if not args.no_plain and rank == 0:
+        psteps = 10
+        tot_ms, tot_units = 0.0, 0
+        for e in ens:
+            st = e.states[0]
+            from remd_b200 import systems as S
+            one = E.REMDGPU([S.Ensemble("p", e.spec, 1, 1, e.T[:1], e.P[:1], [st])],
+                            precision="fp64", device=dev, interval=psteps)
+            s1 = torch.cuda.ExternalStream(E.lib().remd_stream(one.h))
+            one.execute_async(e.T[:1], e.P[:1])
+            one.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s1)
+            one.execute_async()
+            b.record(s1)
+            one.synchronize()
+            tot_ms += a.elapsed_time(b)
+            tot_units += e.spec.nmol * psteps
+            one.close()
+        plain = {"value": tot_units / (tot_ms * 1e-3), "unit": METRIC, "dtype": "f64",
+                 "sample": f"one replica of each of the {len(ens)} ensembles, alone, "
+                           f"{psteps} steps each (one launch sequence per replica)"}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        nst = args.cpu_steps or 2
+        cpu = cpu_baseline(ens, nst, cpu_threads())
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": workload_desc(args.config, ens, args.interval),
+                "gpu_launches": eng.launches_per_interval() * args.steps,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "plain_fp64": plain,
+                "speedup_vs_plain_fp64": (value / world / plain["value"]) if plain else None,
+                "wall_s": wall, "interval_ms": [round(x, 3) for x in ms],
+                "replica_status_nonzero": int(sum(1 for s in statuses if s))}
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            engine_arm(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

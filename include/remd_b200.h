@@ -1,0 +1,275 @@
+/*
+ * remd_b200.h -- C-ABI of the B200 REMD engine (libremd_b200.so).
+ *
+ * The engine replaces the reference's GPU engine, class REMDGPU
+ * (src/remdgpu.h:92-238), and the CPU surface the REMD driver uses on the hot
+ * path (Molecules::ExecuteSteps / GetAverage / ChangeTemperature ...,
+ * src/molecules.h:305-402).  Every call returns a remd_status; none exits the
+ * process (the reference calls exit(EXIT_FAILURE), src/remdgpu.cu:208-212).
+ *
+ * Units are the reference's reduced units (src/unit.h:1-19): length A, energy
+ * kJ/mol, mass 15.9994 g/mol, time sqrt(m A^2 / E); temperatures and pressures
+ * passed in and out are reduced (T/unit_temp, P/unit_press), exactly what
+ * REMDInfo::temperature / pressure hold (src/remdinfo.cxx:167-170).
+ *
+ * Replica state uses Molecules' internal convention after ReadCheckPoint
+ * (src/io_manager.cxx:580-585): r is the box fraction in [0,1), v is the
+ * velocity multiplied by L*s, p the conjugate quaternion momentum multiplied
+ * by s.
+ *
+ * Threading: one handle is used by one host thread at a time.  Device work is
+ * issued on the handle's own CUDA stream; calls that return host data
+ * synchronise that stream.
+ */
+#ifndef REMD_B200_H
+#define REMD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  REMD_OK = 0,
+  REMD_ERR_INVALID = 1,        /* bad argument or unsupported combination            */
+  REMD_ERR_OOM = 2,            /* device allocation or HBM budget exceeded           */
+  REMD_ERR_TIMEOUT = 3,        /* a bounded wait ran out                             */
+  REMD_ERR_NONFINITE = 4,      /* a replica produced NaN/Inf (see remd_replica_status)*/
+  REMD_ERR_CANCELLED = 5,      /* job cancelled                                      */
+  REMD_ERR_CUDA = 6,           /* CUDA runtime error (message in remd_last_error)    */
+  REMD_ERR_IO = 7,             /* file could not be read or written                  */
+  REMD_ERR_NEIGHBOR_OVERFLOW = 8, /* a neighbour list exceeded its capacity          */
+  REMD_ERR_NO_DEVICE = 9       /* no CUDA device                                     */
+} remd_status;
+
+#define REMD_NUM_AVERAGES 19   /* Average::NUM_ELEM, src/remdinfo.h:29-41 */
+#define REMD_MAX_SITES 5
+
+/* Average field order (src/remdinfo.h:29-41): */
+enum {
+  REMD_AVG_LJ = 0, REMD_AVG_CLMB, REMD_AVG_WALL, REMD_AVG_VOL, REMD_AVG_TRA, REMD_AVG_ROT,
+  REMD_AVG_T, REMD_AVG_P, REMD_AVG_PX, REMD_AVG_PY, REMD_AVG_PZ, REMD_AVG_TOT, REMD_AVG_DRF,
+  REMD_AVG_TSTS, REMD_AVG_TSTV, REMD_AVG_BSTX, REMD_AVG_BSTY, REMD_AVG_BSTZ, REMD_AVG_DUMMY
+};
+
+/* Force arithmetic of a handle. */
+typedef enum {
+  REMD_PREC_FP32 = 0,   /* FP32 pair math, FP64 per-molecule/replica accumulation */
+  REMD_PREC_FP64 = 1    /* all-FP64 (the plain form)                            */
+} remd_precision;
+
+/* One REMD system (an "ensemble"): the Parameter fields on the path
+ * (src/parameter.h:9-300) plus its molecule type as read from moltype.txt
+ * (src/molecules.cxx:69-131; A, g/mol, A, kJ/mol, e).  Site 0 must be the only
+ * Lennard-Jones site (water oxygen); the charged sites must be contiguous and
+ * end at the last site. */
+typedef struct {
+  int nmol;
+  int nsite;
+  double site_r[REMD_MAX_SITES][3];
+  double site_mass[REMD_MAX_SITES];
+  double site_sigma[REMD_MAX_SITES];
+  double site_eps[REMD_MAX_SITES];
+  double site_charge[REMD_MAX_SITES];
+  int tconstant;            /* 0 NVE-like, 1 Nose-Poincare                       */
+  int pconstant;            /* 0 none, 1 3-D, 2 z (tube), 3 xy (slit)            */
+  int confined;             /* 0 bulk, 1 nanotube, 2 nano-slit                   */
+  double dt_fs;
+  double rcut, rswitch;     /* A */
+  int nfwall;
+  double wall_length;       /* A: tube radius or slit width                       */
+  double sgm_wall, eps_wall, rho_wall;
+  int interval;             /* MD steps per ExecuteSteps call                    */
+} remd_system_desc;
+
+/* Initial state of one replica (borrowed for the duration of the call). */
+typedef struct {
+  const double *r;          /* nmol*3 box fraction                               */
+  const double *v;          /* nmol*3 velocity * L * s                           */
+  const double *q;          /* nmol*4 unit quaternion                            */
+  const double *p;          /* nmol*4 conjugate momentum * s                     */
+  const double *mass;       /* nmol   reduced mass (the .chk "m" column)         */
+  const double *inertia;    /* nmol*3 principal moments (the .chk "I" columns)   */
+  double s, Ps, Q;          /* Thermostat, src/variables.h:260-271               */
+  double Pv[3], W;          /* Barostat, src/variables.h:273-280                 */
+  double L[3];              /* box lengths, A                                    */
+  double T, P;              /* reduced condition                                 */
+} remd_replica_init;
+
+/* Mutable view filled by remd_get_state (caller-owned arrays, any may be NULL). */
+typedef struct {
+  double *r, *v, *q, *p;    /* as remd_replica_init                              */
+  double *f;                /* nmol*3 molecular force of the last force call      */
+  double *n;                /* nmol*4 body torque 4-vector (src/molecules.cxx:409-418) */
+  double s, Ps, Q, Pv[3], W, L[3], T, P, H0;
+  double pot, lj, clmb, wall, vir[3];
+} remd_state_view;
+
+typedef struct remd_engine_s *remd_handle;
+
+/* ---- engine lifetime ------------------------------------------------------ */
+
+/* Replaces REMDGPU::REMDGPU(Molecules**, nreplica) (src/remdgpu.cu:178-503).
+ * nens systems; reps_per_ens[e] replicas of system e, their states in order in
+ * reps.  Computes the initial forces and H0 (the reference's dt=0 pass,
+ * src/remdgpu.cu:461-478).  All systems must share `interval`. */
+remd_status remd_create(const remd_system_desc *systems, int nens, const int *reps_per_ens,
+                        const remd_replica_init *reps, remd_precision prec, int device,
+                        remd_handle *out);
+
+/* Replaces REMDGPU::~REMDGPU. */
+remd_status remd_destroy(remd_handle h);
+
+/* Replaces REMDGPU::ExecuteSteps(double* T, double* P) (src/remdgpu.cu:656-681):
+ * advance every replica by `interval` steps under the given reduced conditions
+ * (length = total replicas).  A replica whose T or P differs from its previous
+ * condition first gets the reference's exchange tail (ChangeTemperature,
+ * KillMomentum, SetPressure, CalcProperties, UpdateHamiltonian,
+ * src/remd.cxx:526-536). */
+remd_status remd_execute_steps(remd_handle h, const double *T, const double *P);
+
+/* Same, with the conditions already on the device and without the trailing
+ * copy of the averages (used by remd_run_remd and the benchmark). */
+remd_status remd_execute_steps_async(remd_handle h, const double *T, const double *P);
+remd_status remd_synchronize(remd_handle h);
+
+/* Replaces REMDGPU::GetAverages(rep) (src/remdgpu.h:208-233): the 19 fields of
+ * Average for replica `rep` after the last ExecuteSteps (T and P reduced). */
+remd_status remd_get_averages(remd_handle h, int rep, double out[REMD_NUM_AVERAGES]);
+/* All replicas at once: out is nrep*19. */
+remd_status remd_get_all_averages(remd_handle h, double *out);
+
+/* Replaces REMDGPU::ConvertVariablesToHost (src/remdgpu.cu:806-854). */
+remd_status remd_get_state(remd_handle h, int rep, remd_state_view *out);
+
+/* Recompute forces (no integration) and return them through remd_get_state:
+ * the snapshot used by the parity tests (Molecules::CalcForcePot). */
+remd_status remd_compute_forces(remd_handle h);
+
+/* Totals and per-replica information. */
+int remd_num_replicas(remd_handle h);
+int remd_replica_nmol(remd_handle h, int rep);
+/* Unordered molecule pairs within rcut evaluated by the last force call, summed
+ * over replicas (integer reduction; the roofline's pair count). */
+long long remd_last_pair_count(remd_handle h);
+/* Number of the engine's kernels launched per ExecuteSteps call. */
+int remd_launches_per_interval(remd_handle h);
+
+/* Unordered pairs within rcut of one replica in the last force call. */
+long long remd_replica_pair_count(remd_handle h, int rep);
+
+/* The handle's CUDA stream (a cudaStream_t), for timing with CUDA events. */
+void *remd_stream(remd_handle h);
+
+/* Timing pass: runs nsteps MD steps launching the kernels one by one (no
+ * graph) with CUDA events around each launch, and returns the mean device
+ * time in ms of {integrate, force} launches in ms_out[0..1].  The state
+ * advances like remd_execute_steps minus the interval start/end kernels'
+ * bookkeeping (use on a scratch handle). */
+remd_status remd_profile_steps(remd_handle h, int nsteps, double *ms_out);
+
+/* FP32 FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) from a register-
+ * resident FMA-chain kernel over every SM; the denominator of the force
+ * kernel's roofline. */
+remd_status remd_measure_fp32_peak(int device, double *tflops);
+
+/* Per-replica health word of the last interval: 0 ok, else a remd_status. */
+remd_status remd_replica_status(remd_handle h, int rep, int *status);
+
+/* Tuning: atoms of one force tile (32..256, multiple of 32) and the neighbour
+ * skin (A).  Takes effect on the next call. */
+remd_status remd_set_tuning(remd_handle h, int tile, double skin);
+
+/* ---- exchange (src/remd.cxx:467-538, src/remdinfo.cxx:54-125) ------------- */
+
+/* REMD::ReplicaExchange for one ensemble on the host: index (condition slot ->
+ * replica), temperature/pressure (per replica) are updated in place; u[i] is
+ * the uniform compared with exp(-delta) for pair i of list step%4.  Writes the
+ * accept flags (length ntemp*npress/2) and returns the pair count in *npairs. */
+remd_status remd_exchange_host(int ntemp, int npress, int pconstant, long step, int *index,
+                               double *temperature, double *pressure, const double *pot,
+                               const double *vol, const double *u, int *accepted,
+                               int *npairs);
+
+/* The same decision for every ensemble of a handle, on the device, fed by the
+ * potential energies and volumes of the last interval.  u holds, per ensemble,
+ * ntemp*npress/2 uniforms (concatenated); pass NULL to draw them from a
+ * counter-based Philox stream seeded with `seed`.  grids gives ntemp,npress per
+ * ensemble (2*nens ints).  Conditions take effect on the next
+ * remd_execute_steps_device call. */
+remd_status remd_exchange_device(remd_handle h, const int *grids, long step, const double *u,
+                                 unsigned long long seed);
+/* Advance one interval with the conditions left on the device by
+ * remd_exchange_device (no host round trip). */
+remd_status remd_execute_steps_device(remd_handle h);
+/* Read back the device-side condition arrays (index per ensemble slot, T, P per replica). */
+remd_status remd_get_conditions(remd_handle h, int *index, double *T, double *P);
+
+/* ---- host-side formats ----------------------------------------------------- */
+
+/* ForceCalculator::CalcWallForce (src/force_calculator.cxx:117-200): the
+ * nfwall x {f, U} wall table the engine builds at create. */
+remd_status remd_wall_table(int confined, int nfwall, double wall_length, double sgm_wall,
+                            double eps_wall, double rho_wall, double *out);
+
+/* IOManager::ReadCheckPoint (src/io_manager.cxx:528-591): reads a .chk into
+ * caller arrays sized for nmol (r, v, q, p, mass, inertia converted like the
+ * reference; scal = s Ps Q Pv0 Pv1 Pv2 W L0 L1 L2). */
+remd_status remd_read_chk(const char *path, int nmol, double *r, double *v, double *q, double *p,
+                          double *mass, double *inertia, double *scal);
+/* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) of replica rep. */
+remd_status remd_write_chk(remd_handle h, int rep, const char *path);
+
+/* Text of the last error on this thread. */
+const char *remd_last_error(void);
+/* Library version string. */
+const char *remd_version(void);
+
+/* ---- serving: continuous batching of REMD jobs ----------------------------- */
+
+typedef struct remd_server_s *remd_server;
+typedef long long remd_job_id;
+
+typedef struct {
+  remd_system_desc system;
+  int ntemp, npress;
+  const remd_replica_init *reps;   /* ntemp*npress states, copied at submit */
+  int ninterval;                   /* intervals to run                       */
+  unsigned long long seed;         /* exchange stream                        */
+} remd_job_desc;
+
+typedef struct {
+  int state;                 /* 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
+  int intervals_done;
+  double submit_s, start_s, end_s;   /* server clock, seconds */
+  remd_status status;
+} remd_job_info;
+
+typedef struct {
+  long long jobs_done, intervals_done, mol_steps;
+  double p50_interval_ms, p99_interval_ms;   /* per batched interval */
+  double p50_job_s, p99_job_s;               /* submit -> done       */
+  double busy_s;
+  long long bytes_in_use, budget_bytes;
+} remd_server_stats;
+
+remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision prec,
+                             remd_server *out);
+remd_status remd_server_close(remd_server s);
+remd_status remd_job_submit(remd_server s, const remd_job_desc *job, remd_job_id *id);
+remd_status remd_job_poll(remd_server s, remd_job_id id, remd_job_info *info);
+remd_status remd_job_cancel(remd_server s, remd_job_id id);
+/* Final averages (ntemp*npress*19) and the condition index of a finished job. */
+remd_status remd_job_result(remd_server s, remd_job_id id, double *averages, int *index);
+/* Run one scheduling round: admit queued jobs while the budget allows, then
+ * advance every admitted job by one interval as one batch.  Returns the number
+ * of jobs still queued or running in *pending. */
+remd_status remd_server_step(remd_server s, int *pending);
+remd_status remd_server_stats_get(remd_server s, remd_server_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* REMD_B200_H */

@@ -1,0 +1,213 @@
+// ref_driver.cxx -- a C-ABI around the reference's own CPU objects
+// (Molecules, ForceCalculator, integrator, REMDInfo), compiled unmodified from
+// the reference's src/ by oracle/Makefile into oracle/_ref/libremdref*.so.
+//
+// TEST INFRASTRUCTURE ONLY: it pins the C restatement (remd_oracle.c) and is
+// the timed CPU baseline in bench.py.  The engine never links it.
+//
+// The reference's .chk reader (src/io_manager.cxx:528-591) cannot be compiled
+// (it needs the unvendored VMD molfile plugin), so the caller passes the state
+// arrays already converted the way ReadCheckPoint converts them: r as a box
+// fraction, v scaled by L*s, p scaled by s.
+#include "molecules.h"
+#include "remdinfo.h"
+
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+struct RefHandle {
+  Parameter param;
+  Molecules* m = nullptr;
+};
+}  // namespace
+
+extern "C" {
+
+void* ref_create(const char* inp_text) {
+  auto* h = new RefHandle;
+  std::istringstream is(inp_text);
+  h->param.read(is);
+  h->m = new Molecules(h->param);
+  return h;
+}
+
+// ForceCalculator's destructor frees `fwall` even when it was never allocated
+// (bulk systems, src/force_calculator.cxx:54-110), so a Molecules object is
+// deliberately leaked rather than deleted.
+void ref_destroy(void* hp) { (void)hp; }
+
+int ref_natom(void* hp) { return static_cast<RefHandle*>(hp)->m->natom; }
+
+void ref_set_state(void* hp, const double* r, const double* v, const double* q,
+                   const double* p, const double* mass, const double* I, double s,
+                   double Ps, double Q, const double* Pv, double W, const double* L) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  int id = 0;
+  for (int i = 0; i < m->nmol; i++) {
+    Molecule& a = m->mlcl[i];
+    for (int d = 0; d < 3; d++) {
+      a.r[d] = r[3 * i + d];
+      a.v[d] = v[3 * i + d];
+      a.i[d] = I[3 * i + d];
+    }
+    for (int d = 0; d < 4; d++) {
+      a.q[d] = q[4 * i + d];
+      a.p[d] = p[4 * i + d];
+    }
+    a.m = mass[i];
+    a.type = 0;
+    a.id = id;
+    id += m->mlist[0].a.size();
+  }
+  m->tst->s = s;
+  m->tst->Ps = Ps;
+  m->tst->Q = Q;
+  for (int d = 0; d < 3; d++) {
+    m->bst->Pv[d] = Pv[d];
+    m->L[d] = L[d];
+  }
+  m->bst->W = W;
+}
+
+// scal: s Ps Q Pv0 Pv1 Pv2 W L0 L1 L2 T P gkT H0
+void ref_get_state(void* hp, double* r, double* v, double* q, double* p, double* f,
+                   double* n, double* scal) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  for (int i = 0; i < m->nmol; i++) {
+    const Molecule& a = m->mlcl[i];
+    for (int d = 0; d < 3; d++) {
+      if (r) r[3 * i + d] = a.r[d];
+      if (v) v[3 * i + d] = a.v[d];
+      if (f) f[3 * i + d] = a.f[d];
+    }
+    for (int d = 0; d < 4; d++) {
+      if (q) q[4 * i + d] = a.q[d];
+      if (p) p[4 * i + d] = a.p[d];
+      if (n) n[4 * i + d] = a.n[d];
+    }
+  }
+  if (scal) {
+    scal[0] = m->tst->s;
+    scal[1] = m->tst->Ps;
+    scal[2] = m->tst->Q;
+    for (int d = 0; d < 3; d++) scal[3 + d] = m->bst->Pv[d];
+    scal[6] = m->bst->W;
+    for (int d = 0; d < 3; d++) scal[7 + d] = m->L[d];
+    scal[10] = m->T;
+    scal[11] = m->P;
+    scal[12] = m->prop.gkT;
+    scal[13] = m->prop.H0;
+  }
+}
+
+// out: pot lj clmb wall vir0 vir1 vir2 tra rot kin T prs0 prs1 prs2 prs3 tst bst tot ham H0 gkT
+void ref_get_property(void* hp, double* out) {
+  const Property& pr = static_cast<RefHandle*>(hp)->m->prop;
+  const double vals[] = {pr.pot,   pr.lj,     pr.clmb,   pr.wall,   pr.vir[0], pr.vir[1], pr.vir[2],
+                         pr.tra,   pr.rot,    pr.kin,    pr.T,      pr.prs[0], pr.prs[1], pr.prs[2],
+                         pr.prs[3], pr.tst,   pr.bst,    pr.tot,    pr.ham,    pr.H0,     pr.gkT};
+  std::memcpy(out, vals, sizeof(vals));
+}
+
+void ref_get_average(void* hp, double* out) {
+  Average a = static_cast<RefHandle*>(hp)->m->GetAverage();
+  for (int i = 0; i < Average::NUM_ELEM; i++) out[i] = a.sum[i];
+}
+
+void ref_get_fwall(void* hp, double* out) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  for (int i = 0; i < m->fclcltr->nfwall; i++) {
+    out[2 * i] = m->fclcltr->fwall[i][0];
+    out[2 * i + 1] = m->fclcltr->fwall[i][1];
+  }
+}
+
+void ref_set_temperature(void* hp, double T) { static_cast<RefHandle*>(hp)->m->SetTemperature(T); }
+void ref_set_pressure(void* hp, double P) { static_cast<RefHandle*>(hp)->m->SetPressure(P); }
+void ref_set_tstat_mass(void* hp, double Q) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  m->tst->Q = Q;
+  m->tst->flush();
+}
+void ref_initialize_property(void* hp) { static_cast<RefHandle*>(hp)->m->InitializeProperty(); }
+void ref_calc_force(void* hp) { static_cast<RefHandle*>(hp)->m->CalcForcePot(); }
+void ref_calc_properties(void* hp) { static_cast<RefHandle*>(hp)->m->CalcProperties(); }
+void ref_update_hamiltonian(void* hp) { static_cast<RefHandle*>(hp)->m->UpdateHamiltonian(); }
+void ref_velocity_scaling(void* hp) { static_cast<RefHandle*>(hp)->m->VelocityScaling(); }
+void ref_ang_velocity_scaling(void* hp) { static_cast<RefHandle*>(hp)->m->AngVelocityScaling(); }
+void ref_kill_momentum(void* hp) { static_cast<RefHandle*>(hp)->m->KillMomentum(); }
+void ref_change_temperature(void* hp, double T) { static_cast<RefHandle*>(hp)->m->ChangeTemperature(T); }
+
+// Molecules::ExecuteSteps runs param.interval steps then CalcProperties.
+void ref_execute_steps(void* hp, int nsteps) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  m->param.interval = nsteps;
+  m->ExecuteSteps();
+}
+
+// Replica-parallel form: every handle advances nsteps on its own thread, the
+// strongest CPU form of the reference (one replica per core).
+void ref_execute_steps_parallel(void** hs, int nrep, int nsteps, int nthreads) {
+  if (nthreads < 1) nthreads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nthreads; t++) {
+    pool.emplace_back([=]() {
+      for (int r = t; r < nrep; r += nthreads) ref_execute_steps(hs[r], nsteps);
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
+// ---- exchange on top of the reference's compiled REMDInfo ----
+// REMD::ReplicaExchange (src/remd.cxx:486-538) restated with an injected
+// uniform stream in place of rand()/RAND_MAX.
+void* ref_remdinfo_create(const char* inp_text) {
+  Parameter p;
+  std::istringstream is(inp_text);
+  p.read(is);
+  return new REMDInfo(p);
+}
+// REMDInfo's destructor frees its Histogram objects with delete[] on memory
+// from new (src/remdinfo.cxx:296-300), so the handle is deliberately leaked.
+void ref_remdinfo_destroy(void*) {}
+void ref_remdinfo_arrays(void* h, int* index, double* T, double* P) {
+  REMDInfo* ri = static_cast<REMDInfo*>(h);
+  for (int i = 0; i < ri->GetNumReplica(); i++) {
+    if (index) index[i] = ri->GetIndex(i);
+    if (T) T[i] = ri->GetTemperature(i);
+    if (P) P[i] = ri->GetPressure(i);
+  }
+}
+int ref_remdinfo_exchange(void* h, long step, const double* pot, const double* vol,
+                          const double* u, int* accepted) {
+  REMDInfo* ri = static_cast<REMDInfo*>(h);
+  ri->SetAllIsExchangedGlobal(false);
+  const int ec_type = step % 4;
+  const int len = ri->GetListLength(ec_type);
+  for (int i = 0; i < len; ++i) {
+    const Pair pair = ri->GetPair(ec_type, i);
+    const int ind1 = ri->GetIndex(pair.a);
+    const int ind2 = ri->GetIndex(pair.b);
+    const double beta1 = 1. / ri->GetTemperature(ind1);
+    const double beta2 = 1. / ri->GetTemperature(ind2);
+    const double press1 = ri->GetPressure(ind1);
+    const double press2 = ri->GetPressure(ind2);
+    double delta = (beta2 - beta1) * (pot[ind1] - pot[ind2]);
+    if (((ri->GetEnsemble() >> PSHIFT) & MASK) > 0)
+      delta += (beta2 * press2 - beta1 * press1) * (vol[ind1] - vol[ind2]);
+    if (exp(-delta) > u[i]) {
+      ri->ExchangeAccepted(ec_type, i);
+      accepted[i] = 1;
+    } else {
+      ri->ExchangeRejected(ec_type, i);
+      accepted[i] = 0;
+    }
+  }
+  return len;
+}
+
+}  // extern "C"

@@ -1,0 +1,742 @@
+// engine.cu -- host side of the B200 REMD engine: validation, device layout,
+// the CUDA-graph interval, and the C-ABI entry points of include/remd_b200.h
+// that replace class REMDGPU (src/remdgpu.h:92-238).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/remd_b200.h"
+#include "engine_types.cuh"
+#include "hostio.h"
+#include "kernels.cuh"
+
+using namespace remd;
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));               \
+      return REMD_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+struct remd_engine_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int prec = kF32;
+  int tile = 128;
+  double skin = 1.0;
+  int nens = 0, nrep = 0, N = 0, interval = 0;
+  std::vector<remd_system_desc> sys;
+  std::vector<int> rep_ens, ens_rep_off, ens_nrep;
+  std::vector<RepConst> rc;
+  std::vector<Tile> tiles;
+  std::vector<double> curT, curP;
+  std::vector<double> wall_h;
+  DevPtrs d{};
+  RepState *X = nullptr, *Y = nullptr;
+  void* pool = nullptr;           // one device allocation holds every array
+  size_t pool_bytes = 0;
+  double *hT = nullptr, *hP = nullptr, *havg = nullptr;   // pinned
+  double *dT = nullptr, *dP = nullptr;                    // device conditions
+  int* d_index = nullptr;                                 // device exchange index (per replica slot)
+  int *d_grid = nullptr, *d_rep_off = nullptr, *d_u_off = nullptr;
+  double* d_u = nullptr;
+  int u_cap = 0;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_tile = 0;
+  long long last_pairs = 0;
+  size_t bytes = 0;
+};
+
+static int valid_model(const remd_system_desc& s, int* c0) {
+  const int ns = s.nsite;
+  if (ns < 3 || ns > 5) return 0;
+  for (int k = 1; k < ns; k++)
+    if (s.site_eps[k] != 0.0) return 0;   // only site 0 is a Lennard-Jones site
+  if (s.site_eps[0] <= 0.0) return 0;
+  int first = -1;
+  for (int k = 0; k < ns; k++)
+    if (s.site_charge[k] != 0.0) { first = k; break; }
+  if (first < 0) return 0;
+  for (int k = first; k < ns; k++)
+    if (s.site_charge[k] == 0.0) return 0;
+  if (!((ns == 3 && first == 0) || (ns >= 4 && first == 1))) return 0;
+  *c0 = first;
+  return 1;
+}
+
+static remd_status check_desc(const remd_system_desc& s, std::string& why) {
+  int c0;
+  if (s.nmol < 2 || s.nmol > 65535) { why = "nmol must be in [2, 65535]"; return REMD_ERR_INVALID; }
+  if (!valid_model(s, &c0)) {
+    why = "molecule type: site 0 must be the only LJ site and the charged sites a contiguous tail "
+          "(TIP3P/TIP4P/TIP5P layout)";
+    return REMD_ERR_INVALID;
+  }
+  if (s.tconstant < 0 || s.tconstant > 1) { why = "tconstant must be 0 or 1"; return REMD_ERR_INVALID; }
+  if (s.pconstant < 0 || s.pconstant > 3) { why = "pconstant must be 0..3"; return REMD_ERR_INVALID; }
+  if (s.confined < 0 || s.confined > 2) { why = "confined must be 0..2"; return REMD_ERR_INVALID; }
+  // src/remd.cxx:35-36
+  if (s.confined == 1 && (s.pconstant == 1 || s.pconstant == 3)) { why = "tube needs pconstant 0 or 2"; return REMD_ERR_INVALID; }
+  if (s.confined == 2 && (s.pconstant == 1 || s.pconstant == 2)) { why = "slit needs pconstant 0 or 3"; return REMD_ERR_INVALID; }
+  if (s.confined > 0 && (s.nfwall < 3 || s.wall_length <= 0.0)) { why = "confined system needs nfwall >= 3 and wall_length > 0"; return REMD_ERR_INVALID; }
+  if (!(s.rcut > s.rswitch) || s.rswitch <= 0.0) { why = "need rcut > rswitch > 0"; return REMD_ERR_INVALID; }
+  if (s.interval < 1) { why = "interval must be >= 1"; return REMD_ERR_INVALID; }
+  if (!(s.dt_fs > 0.0)) { why = "dt must be > 0"; return REMD_ERR_INVALID; }
+  return REMD_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Build RepConst/tiles for the current tile size; returns pool layout size.
+static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
+  const int T = h->tile;
+  h->tiles.clear();
+  long long pack_words = 0, nbr_words = 0;
+  for (int r = 0; r < h->nrep; r++) {
+    RepConst& c = h->rc[r];
+    c.tile_off = (int)h->tiles.size();
+    c.ntile = (c.nmol + T - 1) / T;
+    for (int t = 0; t < c.ntile; t++) {
+      Tile tt;
+      tt.rep = r;
+      tt.start = t * T;
+      tt.count = std::min(T, c.nmol - t * T);
+      tt.pad = 0;
+      h->tiles.push_back(tt);
+    }
+    c.pack_stride = pack_stride(c.nsite, h->prec);
+    c.pack_off = pack_words;
+    pack_words += (long long)c.nmol * c.pack_stride;
+    c.nbr_off = nbr_words;
+    nbr_words += (long long)c.ntile * c.nbr_cap * T;
+  }
+  const size_t N = h->N, nt = h->tiles.size(), nr = h->nrep;
+  const size_t elem = (h->prec == kF32) ? 4 : 8;
+  const size_t sizes[] = {
+      nr * sizeof(RepConst),           // 0 rc
+      nt * sizeof(Tile),               // 1 tiles
+      N * 3 * 8, N * 3 * 8, N * 4 * 8, N * 4 * 8, N * 3 * 8, N * 4 * 8,   // 2..7 r v q p f n
+      (size_t)pack_words * elem,       // 8 pack
+      N * sizeof(int4),                // 9 ref_com
+      nt * 3 * 8,                      // 10 Lbuild
+      (size_t)nbr_words * 2,           // 11 nbr
+      N * 4,                           // 12 nbr_cnt
+      std::max<size_t>(h->wall_h.size(), 2) * 8,   // 13 wall
+      nt * sizeof(Part1), nt * sizeof(Part2),      // 14, 15
+      nr * kNumAvg * 8,                // 16 avg
+      nr * 4, 64,                      // 17 status, 18 err
+      nr * 8, nr * 8,                  // 19 T, 20 P
+      nr * sizeof(RepState), nr * sizeof(RepState),   // 21 X, 22 Y
+      nr * 4,                          // 23 index
+      (size_t)h->nens * 2 * 4, (size_t)h->nens * 4, (size_t)h->nens * 4,   // 24 grid 25 rep_off 26 u_off
+      (size_t)std::max(nr / 2, (size_t)1) * 8,   // 27 u
+  };
+  offs.clear();
+  total = 0;
+  for (size_t s : sizes) {
+    offs.push_back(total);
+    total += align256(s);
+  }
+}
+
+static remd_status allocate(remd_engine_s* h) {
+  std::vector<size_t> offs;
+  size_t total;
+  layout(h, offs, total);
+  if (h->pool) { cudaFree(h->pool); h->pool = nullptr; }
+  cudaError_t e = cudaMalloc(&h->pool, total);
+  if (e != cudaSuccess) {
+    set_error(std::string("device allocation of ") + std::to_string(total) + " bytes: " + cudaGetErrorString(e));
+    return REMD_ERR_OOM;
+  }
+  h->pool_bytes = total;
+  char* b = static_cast<char*>(h->pool);
+  CK(cudaMemsetAsync(b, 0, total, h->stream));
+  DevPtrs& d = h->d;
+  d.N = h->N;
+  d.ntiles = (int)h->tiles.size();
+  d.nrep = h->nrep;
+  d.rc = reinterpret_cast<RepConst*>(b + offs[0]);
+  d.tiles = reinterpret_cast<Tile*>(b + offs[1]);
+  d.r = reinterpret_cast<double*>(b + offs[2]);
+  d.v = reinterpret_cast<double*>(b + offs[3]);
+  d.q = reinterpret_cast<double*>(b + offs[4]);
+  d.p = reinterpret_cast<double*>(b + offs[5]);
+  d.f = reinterpret_cast<double*>(b + offs[6]);
+  d.n = reinterpret_cast<double*>(b + offs[7]);
+  d.pack = b + offs[8];
+  d.ref_com = reinterpret_cast<int4*>(b + offs[9]);
+  d.Lbuild = reinterpret_cast<double*>(b + offs[10]);
+  d.nbr = reinterpret_cast<uint16_t*>(b + offs[11]);
+  d.nbr_cnt = reinterpret_cast<int*>(b + offs[12]);
+  d.wall = reinterpret_cast<double*>(b + offs[13]);
+  d.part1 = reinterpret_cast<Part1*>(b + offs[14]);
+  d.part2 = reinterpret_cast<Part2*>(b + offs[15]);
+  d.avg = reinterpret_cast<double*>(b + offs[16]);
+  d.status = reinterpret_cast<int*>(b + offs[17]);
+  d.err = reinterpret_cast<int*>(b + offs[18]);
+  h->dT = reinterpret_cast<double*>(b + offs[19]);
+  h->dP = reinterpret_cast<double*>(b + offs[20]);
+  d.newT = h->dT;
+  d.newP = h->dP;
+  d.changed = nullptr;
+  h->X = reinterpret_cast<RepState*>(b + offs[21]);
+  h->Y = reinterpret_cast<RepState*>(b + offs[22]);
+  h->d_index = reinterpret_cast<int*>(b + offs[23]);
+  h->d_grid = reinterpret_cast<int*>(b + offs[24]);
+  h->d_rep_off = reinterpret_cast<int*>(b + offs[25]);
+  h->d_u_off = reinterpret_cast<int*>(b + offs[26]);
+  h->d_u = reinterpret_cast<double*>(b + offs[27]);
+  h->u_cap = std::max(h->nrep / 2, 1);
+  h->bytes = total;
+  CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync((void*)d.tiles, h->tiles.data(), h->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, h->stream));
+  if (!h->wall_h.empty())
+    CK(cudaMemcpyAsync((void*)d.wall, h->wall_h.data(), h->wall_h.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  // later set-up copies use the default stream, which does not order with this
+  // non-blocking stream: finish the clear and the uploads first
+  CK(cudaStreamSynchronize(h->stream));
+  return REMD_OK;
+}
+
+static remd_status sync_and_check(remd_engine_s* h) {
+  CK(cudaStreamSynchronize(h->stream));
+  int err = 0;
+  CK(cudaMemcpy(&err, h->d.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err & kErrNbrOverflow) {
+    set_error("neighbour list capacity exceeded");
+    return REMD_ERR_NEIGHBOR_OVERFLOW;
+  }
+  if (err & kErrNonFinite) {
+    set_error("a replica produced a non-finite energy (see remd_replica_status)");
+    return REMD_ERR_NONFINITE;
+  }
+  return REMD_OK;
+}
+
+// Upload SoA state from host copies (component-major).
+static remd_status upload_state(remd_engine_s* h, const std::vector<double>& r, const std::vector<double>& v,
+                                const std::vector<double>& q, const std::vector<double>& p,
+                                const std::vector<RepState>& st) {
+  const size_t N = h->N;
+  CK(cudaMemcpyAsync(h->d.r, r.data(), N * 3 * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d.v, v.data(), N * 3 * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d.q, q.data(), N * 4 * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d.p, p.data(), N * 4 * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->X, st.data(), st.size() * sizeof(RepState), cudaMemcpyHostToDevice, h->stream));
+  return REMD_OK;
+}
+
+static remd_status initial_force(remd_engine_s* h) {
+  launch_pack(h->d, h->prec, h->tile, h->stream);
+  launch_force(h->d, h->X, h->X, h->prec, true, h->tile, h->stream);
+  launch_replica_props(h->d, h->X, h->stream);
+  CK(cudaGetLastError());
+  return sync_and_check(h);
+}
+
+static remd_status build_graph(remd_engine_s* h) {
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  launch_replica_start(h->d, h->X, h->stream);
+  for (int s = 0; s < h->interval; s++) {
+    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
+  }
+  launch_replica_end(h->d, h->X, h->stream);
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+  if (le != cudaSuccess || ce != cudaSuccess) {
+    set_error(std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ce));
+    return REMD_ERR_CUDA;
+  }
+  cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    set_error(std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    return REMD_ERR_CUDA;
+  }
+  h->graph_tile = h->tile;
+  return REMD_OK;
+}
+
+static long long host_pairs(remd_engine_s* h) {
+  std::vector<Part2> p2(h->tiles.size());
+  if (cudaMemcpy(p2.data(), h->d.part2, p2.size() * sizeof(Part2), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  long long s = 0;
+  for (auto& p : p2) s += p.npairs;
+  return s / 2;
+}
+
+extern "C" {
+
+remd_status remd_create(const remd_system_desc* systems, int nens, const int* reps_per_ens,
+                        const remd_replica_init* reps, remd_precision prec, int device,
+                        remd_handle* out) {
+  if (!systems || nens < 1 || !reps_per_ens || !reps || !out) {
+    set_error("remd_create: null argument");
+    return REMD_ERR_INVALID;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    set_error("no CUDA device");
+    return REMD_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) { set_error("bad device"); return REMD_ERR_INVALID; }
+  std::string why;
+  for (int e = 0; e < nens; e++) {
+    remd_status st = check_desc(systems[e], why);
+    if (st != REMD_OK) { set_error("system " + std::to_string(e) + ": " + why); return st; }
+    if (systems[e].interval != systems[0].interval) {
+      set_error("all systems of one handle must share `interval`");
+      return REMD_ERR_INVALID;
+    }
+    if (reps_per_ens[e] < 1) { set_error("reps_per_ens must be >= 1"); return REMD_ERR_INVALID; }
+  }
+  auto* h = new remd_engine_s;
+  h->device = device;
+  h->prec = (prec == REMD_PREC_FP64) ? kF64 : kF32;
+  h->nens = nens;
+  h->interval = systems[0].interval;
+  h->sys.assign(systems, systems + nens);
+  // wall tables, one per ensemble
+  std::vector<int> wall_off(nens, 0);
+  for (int e = 0; e < nens; e++) {
+    const remd_system_desc& s = systems[e];
+    if (s.confined > 0) {
+      wall_off[e] = (int)(h->wall_h.size() / 2);
+      std::vector<double> t(2 * (size_t)s.nfwall);
+      wall_table(s.confined, s.nfwall, s.wall_length, s.sgm_wall, s.eps_wall, s.rho_wall, t.data());
+      h->wall_h.insert(h->wall_h.end(), t.begin(), t.end());
+    }
+  }
+  // replicas
+  int rep = 0, mol = 0;
+  std::vector<RepState> st0;
+  for (int e = 0; e < nens; e++) {
+    const remd_system_desc& s = systems[e];
+    h->ens_rep_off.push_back(rep);
+    h->ens_nrep.push_back(reps_per_ens[e]);
+    int c0 = 0;
+    valid_model(s, &c0);
+    for (int k = 0; k < reps_per_ens[e]; k++, rep++) {
+      const remd_replica_init& ri = reps[rep];
+      if (!ri.r || !ri.v || !ri.q || !ri.p || !ri.mass || !ri.inertia) {
+        set_error("replica " + std::to_string(rep) + ": null state array");
+        delete h;
+        return REMD_ERR_INVALID;
+      }
+      for (int i = 1; i < s.nmol; i++) {
+        if (ri.mass[i] != ri.mass[0] || ri.inertia[3 * i] != ri.inertia[0] ||
+            ri.inertia[3 * i + 1] != ri.inertia[1] || ri.inertia[3 * i + 2] != ri.inertia[2]) {
+          set_error("replica " + std::to_string(rep) + ": molecules of one replica must share mass and inertia");
+          delete h;
+          return REMD_ERR_INVALID;
+        }
+      }
+      if (!(ri.Q > 0.0) || (s.pconstant > 0 && !(ri.W > 0.0)) || !(ri.T > 0.0) ||
+          !(ri.L[0] > 0 && ri.L[1] > 0 && ri.L[2] > 0) || !(ri.s > 0.0)) {
+        set_error("replica " + std::to_string(rep) + ": need Q > 0, W > 0 (barostat), T > 0, L > 0, s > 0");
+        delete h;
+        return REMD_ERR_INVALID;
+      }
+      RepConst c;
+      std::memset(&c, 0, sizeof(c));
+      c.nmol = s.nmol;
+      c.mol_off = mol;
+      c.nsite = s.nsite;
+      c.c0 = c0;
+      c.confined = s.confined;
+      c.tconstant = s.tconstant;
+      c.pconstant = s.pconstant;
+      c.nfwall = s.nfwall;
+      c.wall_off = wall_off[e];
+      c.ens = e;
+      c.dt = s.dt_fs * 1e-15 / unit_time();
+      c.dthalf = s.dt_fs * 1e-15 / unit_time() * 0.5;
+      c.rc = s.rcut;
+      c.rs = s.rswitch;
+      const double rlc = s.rswitch - s.rcut;
+      c.coef_sw = 1.0 / (rlc * rlc * rlc * rlc * rlc);
+      c.skin = h->skin;
+      c.Q = ri.Q;
+      c.W = ri.W > 0.0 ? ri.W : 1.0;
+      c.mass = ri.mass[0];
+      for (int x = 0; x < 3; x++) c.I[x] = ri.inertia[x];
+      const double wl = s.wall_length * 1e-10 / unit_length();
+      c.wall_dr = (s.confined == 2) ? 0.5 * (wl / (double)s.nfwall) : wl / (double)std::max(s.nfwall, 1);
+      c.wall_length_param = s.wall_length;
+      const double sigma_c = 3.4;
+      const double wa = (s.wall_length - 0.5 * sigma_c) * 1e-10 / unit_length();
+      c.bottom_area = M_PI * wa * wa;
+      c.slit_width = s.wall_length * 1e-10 / unit_length();
+      double qr[kMaxSites];
+      for (int k = 0; k < s.nsite; k++) {
+        for (int x = 0; x < 3; x++) c.body[k][x] = s.site_r[k][x] * (1e-10 / unit_length());
+        qr[k] = s.site_charge[k] * (1.6021761e-19 / unit_coulomb());
+      }
+      for (int k = 0; k < s.nsite; k++)
+        for (int l = 0; l < s.nsite; l++) c.qq[k][l] = qr[k] * qr[l];
+      const double sg = 0.5 * (s.site_sigma[0] * (1e-10 / unit_length()) * 2.0);
+      c.sgm2 = sg * sg;
+      const double eo = s.site_eps[0] * (1e+03 / 6.0221367e+23 / unit_energy());
+      c.eps = std::sqrt(eo * eo);
+      const double rl = s.rcut + h->skin;
+      const double cap = 0.1 * 4.0 / 3.0 * M_PI * rl * rl * rl;
+      c.nbr_cap = std::min(s.nmol - 1, ((int)std::ceil(cap) + 7) / 8 * 8);
+      if (c.nbr_cap < 1) c.nbr_cap = 1;
+      h->rc.push_back(c);
+      h->rep_ens.push_back(e);
+      RepState rs;
+      std::memset(&rs, 0, sizeof(rs));
+      rs.s = ri.s;
+      rs.Ps = ri.Ps;
+      for (int x = 0; x < 3; x++) { rs.Pv[x] = ri.Pv[x]; rs.L[x] = ri.L[x]; }
+      rs.T = ri.T;
+      rs.P = ri.P;
+      rs.gkT = 6.0 * s.nmol * ri.T;
+      st0.push_back(rs);
+      h->curT.push_back(ri.T);
+      h->curP.push_back(ri.P);
+      mol += s.nmol;
+    }
+  }
+  h->nrep = rep;
+  h->N = mol;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cannot set up device/stream");
+    delete h;
+    return REMD_ERR_CUDA;
+  }
+  remd_status st = allocate(h);
+  if (st != REMD_OK) { remd_destroy(h); return st; }
+  // host SoA staging
+  const int N = h->N;
+  std::vector<double> r((size_t)N * 3), v((size_t)N * 3), q((size_t)N * 4), p((size_t)N * 4);
+  for (int k = 0; k < h->nrep; k++) {
+    const remd_replica_init& ri = reps[k];
+    const RepConst& c = h->rc[k];
+    for (int i = 0; i < c.nmol; i++) {
+      const int g = c.mol_off + i;
+      for (int x = 0; x < 3; x++) { r[(size_t)x * N + g] = ri.r[3 * i + x]; v[(size_t)x * N + g] = ri.v[3 * i + x]; }
+      for (int x = 0; x < 4; x++) { q[(size_t)x * N + g] = ri.q[4 * i + x]; p[(size_t)x * N + g] = ri.p[4 * i + x]; }
+    }
+  }
+  if ((st = upload_state(h, r, v, q, p, st0)) != REMD_OK) { remd_destroy(h); return st; }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) { set_error("state upload failed"); remd_destroy(h); return REMD_ERR_CUDA; }
+  if (cudaMallocHost(&h->hT, h->nrep * 8) != cudaSuccess || cudaMallocHost(&h->hP, h->nrep * 8) != cudaSuccess ||
+      cudaMallocHost(&h->havg, (size_t)h->nrep * kNumAvg * 8) != cudaSuccess) {
+    set_error("pinned host allocation failed");
+    remd_destroy(h);
+    return REMD_ERR_OOM;
+  }
+  // device-side exchange bookkeeping: identity index, current conditions
+  {
+    std::vector<int> idx(h->nrep), grid(2 * nens), roff(nens), uoff(nens);
+    for (int e = 0; e < nens; e++) {
+      roff[e] = h->ens_rep_off[e];
+      for (int k = 0; k < h->ens_nrep[e]; k++) idx[roff[e] + k] = k;
+    }
+    if (cudaMemcpy(h->d_index, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->dT, h->curT.data(), h->nrep * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->dP, h->curP.data(), h->nrep * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d_rep_off, roff.data(), roff.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("upload of the condition arrays failed");
+      remd_destroy(h);
+      return REMD_ERR_CUDA;
+    }
+  }
+  if ((st = initial_force(h)) != REMD_OK) { remd_destroy(h); return st; }
+  h->last_pairs = host_pairs(h);
+  *out = h;
+  return REMD_OK;
+}
+
+remd_status remd_destroy(remd_handle h) {
+  if (!h) return REMD_OK;
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->pool) cudaFree(h->pool);
+  if (h->hT) cudaFreeHost(h->hT);
+  if (h->hP) cudaFreeHost(h->hP);
+  if (h->havg) cudaFreeHost(h->havg);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return REMD_OK;
+}
+
+remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
+  if (!h || tile < 32 || tile > 256 || tile % 32 || !(skin > 0.0)) {
+    set_error("remd_set_tuning: tile must be 32..256 (multiple of 32), skin > 0");
+    return REMD_ERR_INVALID;
+  }
+  if (tile == h->tile && skin == h->skin) return REMD_OK;
+  // re-lay out the arrays for the new tile, preserving state
+  const int N = h->N;
+  std::vector<double> r((size_t)N * 3), v((size_t)N * 3), q((size_t)N * 4), p((size_t)N * 4), f((size_t)N * 3), n((size_t)N * 4);
+  std::vector<RepState> st(h->nrep);
+  std::vector<double> dT(h->nrep), dP(h->nrep);
+  std::vector<int> idx(h->nrep);
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(r.data(), h->d.r, r.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(v.data(), h->d.v, v.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(q.data(), h->d.q, q.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(p.data(), h->d.p, p.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(st.data(), h->X, st.size() * sizeof(RepState), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(dT.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(dP.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  h->tile = tile;
+  h->skin = skin;
+  for (auto& c : h->rc) {
+    c.skin = skin;
+    const double rl = c.rc + skin;
+    const double cap = 0.1 * 4.0 / 3.0 * M_PI * rl * rl * rl;
+    c.nbr_cap = std::max(1, std::min(c.nmol - 1, ((int)std::ceil(cap) + 7) / 8 * 8));
+  }
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  remd_status s = allocate(h);
+  if (s != REMD_OK) return s;
+  if ((s = upload_state(h, r, v, q, p, st)) != REMD_OK) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  std::vector<int> roff(h->nens);
+  for (int e = 0; e < h->nens; e++) roff[e] = h->ens_rep_off[e];
+  CK(cudaMemcpy(h->dT, dT.data(), h->nrep * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->dP, dP.data(), h->nrep * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_index, idx.data(), h->nrep * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_rep_off, roff.data(), roff.size() * 4, cudaMemcpyHostToDevice));
+  // forces are a pure function of positions: recompute, keep H0
+  launch_pack(h->d, h->prec, h->tile, h->stream);
+  launch_force(h->d, h->X, h->X, h->prec, true, h->tile, h->stream);
+  CK(cudaGetLastError());
+  return sync_and_check(h);
+}
+
+remd_status remd_execute_steps_async(remd_handle h, const double* T, const double* P) {
+  if (!h) { set_error("null handle"); return REMD_ERR_INVALID; }
+  if (T && P) {
+    for (int k = 0; k < h->nrep; k++) {
+      if (!(T[k] > 0.0)) { set_error("temperatures must be > 0"); return REMD_ERR_INVALID; }
+      h->hT[k] = T[k];
+      h->hP[k] = P[k];
+    }
+    CK(cudaMemcpyAsync(h->dT, h->hT, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->dP, h->hP, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
+  }
+  if (!h->gexec || h->graph_tile != h->tile) {
+    remd_status s = build_graph(h);
+    if (s != REMD_OK) return s;
+  }
+  CK(cudaGraphLaunch(h->gexec, h->stream));
+  return REMD_OK;
+}
+
+remd_status remd_synchronize(remd_handle h) {
+  if (!h) return REMD_ERR_INVALID;
+  return sync_and_check(h);
+}
+
+remd_status remd_execute_steps(remd_handle h, const double* T, const double* P) {
+  if (!h || !T || !P) { set_error("remd_execute_steps: null argument"); return REMD_ERR_INVALID; }
+  remd_status s = remd_execute_steps_async(h, T, P);
+  if (s != REMD_OK) return s;
+  CK(cudaMemcpyAsync(h->havg, h->d.avg, (size_t)h->nrep * kNumAvg * 8, cudaMemcpyDeviceToHost, h->stream));
+  s = sync_and_check(h);
+  for (int k = 0; k < h->nrep; k++) { h->curT[k] = T[k]; h->curP[k] = P[k]; }
+  return s;
+}
+
+remd_status remd_execute_steps_device(remd_handle h) {
+  remd_status s = remd_execute_steps_async(h, nullptr, nullptr);
+  if (s != REMD_OK) return s;
+  CK(cudaMemcpyAsync(h->havg, h->d.avg, (size_t)h->nrep * kNumAvg * 8, cudaMemcpyDeviceToHost, h->stream));
+  return sync_and_check(h);
+}
+
+remd_status remd_get_averages(remd_handle h, int rep, double* out) {
+  if (!h || !out || rep < 0 || rep >= h->nrep) { set_error("remd_get_averages: bad argument"); return REMD_ERR_INVALID; }
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(out, h->d.avg + (size_t)rep * kNumAvg, kNumAvg * 8, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+remd_status remd_get_all_averages(remd_handle h, double* out) {
+  if (!h || !out) { set_error("remd_get_all_averages: bad argument"); return REMD_ERR_INVALID; }
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(out, h->d.avg, (size_t)h->nrep * kNumAvg * 8, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+remd_status remd_get_state(remd_handle h, int rep, remd_state_view* o) {
+  if (!h || !o || rep < 0 || rep >= h->nrep) { set_error("remd_get_state: bad argument"); return REMD_ERR_INVALID; }
+  CK(cudaStreamSynchronize(h->stream));
+  const RepConst& c = h->rc[rep];
+  const int n = c.nmol, N = h->N;
+  std::vector<double> tmp((size_t)n);
+  auto pull = [&](const double* src, int ncomp, double* dst) -> remd_status {
+    if (!dst) return REMD_OK;
+    for (int x = 0; x < ncomp; x++) {
+      CK(cudaMemcpy(tmp.data(), src + (size_t)x * N + c.mol_off, n * 8, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; i++) dst[(size_t)ncomp * i + x] = tmp[i];
+    }
+    return REMD_OK;
+  };
+  remd_status s;
+  if ((s = pull(h->d.r, 3, o->r)) != REMD_OK) return s;
+  if ((s = pull(h->d.v, 3, o->v)) != REMD_OK) return s;
+  if ((s = pull(h->d.q, 4, o->q)) != REMD_OK) return s;
+  if ((s = pull(h->d.p, 4, o->p)) != REMD_OK) return s;
+  if ((s = pull(h->d.f, 3, o->f)) != REMD_OK) return s;
+  if ((s = pull(h->d.n, 4, o->n)) != REMD_OK) return s;
+  RepState st;
+  CK(cudaMemcpy(&st, h->X + rep, sizeof(st), cudaMemcpyDeviceToHost));
+  o->s = st.s; o->Ps = st.Ps; o->Q = c.Q; o->W = c.W;
+  for (int x = 0; x < 3; x++) { o->Pv[x] = st.Pv[x]; o->L[x] = st.L[x]; }
+  o->T = st.T; o->P = st.P; o->H0 = st.H0;
+  std::vector<Part2> p2(c.ntile);
+  CK(cudaMemcpy(p2.data(), h->d.part2 + c.tile_off, c.ntile * sizeof(Part2), cudaMemcpyDeviceToHost));
+  double lj = 0, cl = 0, w = 0, v[3] = {0, 0, 0};
+  for (auto& p : p2) { lj += p.lj; cl += p.clmb; w += p.wall; for (int x = 0; x < 3; x++) v[x] += p.vir[x]; }
+  o->lj = lj * 0.5; o->clmb = cl * 0.5; o->wall = w;
+  for (int x = 0; x < 3; x++) o->vir[x] = v[x] * 0.5;
+  o->pot = o->lj + o->clmb + o->wall;
+  return REMD_OK;
+}
+
+remd_status remd_compute_forces(remd_handle h) {
+  if (!h) return REMD_ERR_INVALID;
+  launch_pack(h->d, h->prec, h->tile, h->stream);
+  launch_force(h->d, h->X, h->X, h->prec, true, h->tile, h->stream);
+  CK(cudaGetLastError());
+  remd_status s = sync_and_check(h);
+  h->last_pairs = host_pairs(h);
+  return s;
+}
+
+int remd_num_replicas(remd_handle h) { return h ? h->nrep : 0; }
+int remd_replica_nmol(remd_handle h, int rep) { return (h && rep >= 0 && rep < h->nrep) ? h->rc[rep].nmol : 0; }
+long long remd_last_pair_count(remd_handle h) {
+  if (!h) return -1;
+  cudaStreamSynchronize(h->stream);
+  h->last_pairs = host_pairs(h);
+  return h->last_pairs;
+}
+int remd_launches_per_interval(remd_handle h) { return h ? 2 * h->interval + 2 : 0; }
+
+long long remd_replica_pair_count(remd_handle h, int rep) {
+  if (!h || rep < 0 || rep >= h->nrep) return -1;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return -1;
+  const RepConst& c = h->rc[rep];
+  std::vector<Part2> p2(c.ntile);
+  if (cudaMemcpy(p2.data(), h->d.part2 + c.tile_off, c.ntile * sizeof(Part2), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  long long s = 0;
+  for (auto& p : p2) s += p.npairs;
+  return s / 2;
+}
+
+void* remd_stream(remd_handle h) { return h ? (void*)h->stream : nullptr; }
+
+remd_status remd_profile_steps(remd_handle h, int nsteps, double* ms_out) {
+  if (!h || nsteps < 1 || !ms_out) return REMD_ERR_INVALID;
+  cudaEvent_t ev[3];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double ti = 0.0, tf = 0.0;
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaEventRecord(ev[0], h->stream));
+    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    CK(cudaEventRecord(ev[1], h->stream));
+    launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
+    CK(cudaEventRecord(ev[2], h->stream));
+    CK(cudaEventSynchronize(ev[2]));
+    float a = 0.f, b = 0.f;
+    CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+    ti += a;
+    tf += b;
+  }
+  launch_replica_end(h->d, h->X, h->stream);
+  for (auto& e : ev) cudaEventDestroy(e);
+  ms_out[0] = ti / nsteps;
+  ms_out[1] = tf / nsteps;
+  return sync_and_check(h);
+}
+
+remd_status remd_measure_fp32_peak(int device, double* tflops) {
+  if (!tflops) return REMD_ERR_INVALID;
+  CK(cudaSetDevice(device));
+  double ms = 0.0;
+  long long flops = 0;
+  remd_status s = (remd_status)measure_fp32_fma(device, &ms, &flops);
+  if (s != REMD_OK) return s;
+  *tflops = (double)flops / (ms * 1e-3) / 1e12;
+  return REMD_OK;
+}
+
+remd_status remd_replica_status(remd_handle h, int rep, int* status) {
+  if (!h || !status || rep < 0 || rep >= h->nrep) return REMD_ERR_INVALID;
+  CK(cudaMemcpy(status, h->d.status + rep, 4, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+remd_status remd_exchange_device(remd_handle h, const int* grids, long step, const double* u,
+                                 unsigned long long seed) {
+  if (!h || !grids) { set_error("remd_exchange_device: null argument"); return REMD_ERR_INVALID; }
+  std::vector<int> uoff(h->nens);
+  int tot = 0;
+  for (int e = 0; e < h->nens; e++) {
+    if (grids[2 * e] * grids[2 * e + 1] != h->ens_nrep[e]) {
+      set_error("exchange grid does not match the replica count of ensemble " + std::to_string(e));
+      return REMD_ERR_INVALID;
+    }
+    uoff[e] = tot;
+    tot += exchange_pair_count(grids[2 * e], grids[2 * e + 1], step);
+  }
+  CK(cudaMemcpyAsync(h->d_grid, grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_u_off, uoff.data(), h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  const double* du = nullptr;
+  if (u) {
+    if (tot > h->u_cap) { set_error("too many uniforms"); return REMD_ERR_INVALID; }
+    if (tot > 0) CK(cudaMemcpyAsync(h->d_u, u, tot * 8, cudaMemcpyHostToDevice, h->stream));
+    du = h->d_u;
+  }
+  launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, step, du, seed, h->d_index,
+                    h->dT, h->dP, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));   // host arrays (uoff) go out of scope
+  return REMD_OK;
+}
+
+remd_status remd_get_conditions(remd_handle h, int* index, double* T, double* P) {
+  if (!h) return REMD_ERR_INVALID;
+  CK(cudaStreamSynchronize(h->stream));
+  if (index) CK(cudaMemcpy(index, h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  if (T) CK(cudaMemcpy(T, h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
+  if (P) CK(cudaMemcpy(P, h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+remd_status remd_write_chk(remd_handle h, int rep, const char* path) {
+  if (!h || !path || rep < 0 || rep >= h->nrep) return REMD_ERR_INVALID;
+  const RepConst& c = h->rc[rep];
+  const int n = c.nmol;
+  std::vector<double> r(3 * n), v(3 * n), q(4 * n), p(4 * n);
+  remd_state_view o;
+  std::memset(&o, 0, sizeof(o));
+  o.r = r.data(); o.v = v.data(); o.q = q.data(); o.p = p.data();
+  remd_status s = remd_get_state(h, rep, &o);
+  if (s != REMD_OK) return s;
+  return (remd_status)write_chk(path, n, c.nsite, r.data(), v.data(), q.data(), p.data(), c.mass, c.I,
+                                o.s, o.Ps, o.Q, o.Pv, o.W, o.L);
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// engine_types.cuh -- device data layout of the B200 REMD engine.
+//
+// All replicas of all ensembles of one handle live in one set of arrays:
+//   * molecule state, FP64 structure-of-arrays, component-major
+//     (r[c*N + g], c = 0..2; v likewise; q, p, n with 4 components; f with 3),
+//     g = global molecule index = RepConst::mol_off + local index;
+//   * per-step force records ("pack"), rebuilt by the integrate kernel after
+//     the positions move: FP32 form = {int32 x,y,z fixed-point centre of mass,
+//     float site offsets R(q) b_k} padded to 16 B; FP64 form = {double box
+//     fraction, double site offsets};
+//   * full neighbour lists, uint16 local indices, column-major inside a force
+//     tile so that the lanes of a warp read consecutive words;
+//   * per-replica scalars (thermostat, barostat, box, H0, condition) in two
+//     buffers that the integrate and force kernels ping-pong between;
+//   * per-tile partial sums written by one kernel and reduced, in a fixed
+//     order, by every CTA of the same replica in the next kernel
+//     (deterministic: a replica's result does not depend on its batch mates).
+#pragma once
+#include <cstdint>
+
+namespace remd {
+
+constexpr int kMaxSites = 5;
+constexpr int kNumAvg = 19;
+constexpr double kFix = 4294967296.0;          // 2^32: fixed-point box fraction
+constexpr double kFixInv = 1.0 / 4294967296.0;
+
+// Per-replica constants (read-only on the device).
+struct RepConst {
+  int nmol, mol_off;       // molecules; first global index
+  int tile_off, ntile;     // force/integrate tiles [tile_off, tile_off+ntile)
+  int nsite, c0;           // sites; first charged site (charged sites are [c0, nsite))
+  int confined, tconstant, pconstant;
+  int nfwall, wall_off;    // wall table entries and offset into the table array
+  int nbr_cap;             // neighbour list capacity per molecule
+  int ens;                 // ensemble index
+  int pack_stride;         // words (FP32) or doubles (FP64) per pack record
+  long long pack_off;      // first record word/double of this replica
+  long long nbr_off;       // first neighbour word of tile_off
+  double dt, dthalf;
+  double rc, rs, coef_sw;  // switching: coef_sw = 1/(rs-rc)^5
+  double skin;
+  double Q, W;
+  double mass, I[3];
+  double wall_dr;          // table spacing: wall_length/nfwall (tube) or half of it (slit)
+  double wall_length_param;   // A, as read from .inp
+  double bottom_area;      // GetBottomArea (tube)
+  double slit_width;       // wall length in reduced units (slit volume)
+  double body[kMaxSites][3];
+  double qq[kMaxSites][kMaxSites];
+  double sgm2, eps;        // O-O Lennard-Jones: ((s+s)/2)^2 and sqrt(e e)
+};
+
+// Per-replica scalars (two copies, ping-pong).
+struct RepState {
+  double s, Ps, Pv[3], L[3];
+  double H0, T, P, gkT;
+};
+
+// Integrate-kernel partials of one tile.
+struct Part1 {
+  double sum_Pv[3];
+  double sum_Ps;
+  double disp;             // max |displacement since the list build| (A, build box)
+  double pad[3];
+};
+
+// Force-kernel partials of one tile (raw ordered-pair sums; consumers halve lj/clmb/vir).
+struct Part2 {
+  double lj, clmb, wall, vir[3];
+  long long npairs;        // ordered pairs within rc
+  double pad;
+};
+
+struct Tile {
+  int rep, start, count, pad;   // replica, first local molecule, molecules in tile
+};
+
+// Everything a kernel needs, passed by value.
+struct DevPtrs {
+  int N;                         // total molecules
+  int ntiles, nrep;
+  const RepConst* rc;
+  const Tile* tiles;
+  double *r, *v, *q, *p, *f, *n; // SoA, component-major, stride N
+  void* pack;                    // FP32 words or FP64 doubles
+  int4* ref_com;                 // fixed-point com at the last list build
+  double* Lbuild;                // per tile, 3 doubles (NaN = list invalid)
+  uint16_t* nbr;                 // neighbour lists
+  int* nbr_cnt;                  // per molecule
+  const double* wall;            // {f, U} pairs
+  Part1* part1;
+  Part2* part2;
+  double* avg;                   // nrep * kNumAvg
+  int* status;                   // per replica health word
+  int* err;                      // global error word (bit flags)
+  const double* newT;            // conditions for the next interval (per replica)
+  const double* newP;
+  const int* changed;            // 1 = apply the exchange tail at the interval start
+};
+
+enum : int { kErrNbrOverflow = 1, kErrNonFinite = 2 };
+
+}  // namespace remd

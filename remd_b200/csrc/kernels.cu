@@ -1,0 +1,1038 @@
+// kernels.cu -- device code of the B200 REMD engine.  See kernels.cuh for the
+// step decomposition and engine_types.cuh for the data layout.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "integrator.cuh"
+#include "kernels.cuh"
+
+namespace remd {
+
+int pack_stride(int nsite, int prec) {
+  if (prec == kF32) return ((3 + 3 * nsite) + 3) / 4 * 4;   // words, 16-B multiple
+  return ((3 + 3 * nsite) + 1) / 2 * 2;                      // doubles, 16-B multiple
+}
+
+// ------------------------------------------------------------------ reductions
+template <int K>
+__device__ inline void block_sum(double* v, double* sm) {
+  // deterministic: fixed shuffle tree, then warp partials summed in warp order
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+    for (int k = 0; k < K; k++) sm[warp * K + k] = v[k];
+  __syncthreads();
+  for (int k = 0; k < K; k++) {
+    double t = 0.0;
+    for (int w = 0; w < nw; w++) t += sm[w * K + k];
+    v[k] = t;
+  }
+  __syncthreads();
+}
+
+__device__ inline double block_max(double v, double* sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < nw; w++) t = fmax(t, sm[w]);
+  __syncthreads();
+  return t;
+}
+
+// Sum of the force partials of replica c (ordered pairs -> halved like
+// ForceCalculator::Switching, src/force_calculator.cxx:775-778).
+__device__ inline void reduce_part2(const DevPtrs& d, const RepConst& c, double& lj, double& clmb,
+                                    double& wall, double* vir) {
+  double a = 0, b = 0, w = 0, v0 = 0, v1 = 0, v2 = 0;
+  for (int t = c.tile_off; t < c.tile_off + c.ntile; t++) {
+    const Part2 p = d.part2[t];
+    a += p.lj; b += p.clmb; w += p.wall;
+    v0 += p.vir[0]; v1 += p.vir[1]; v2 += p.vir[2];
+  }
+  lj = a * 0.5;
+  clmb = b * 0.5;
+  wall = w;
+  vir[0] = v0 * 0.5; vir[1] = v1 * 0.5; vir[2] = v2 * 0.5;
+}
+
+// ------------------------------------------------------------------ force records
+__device__ inline int fix_coord(double r) {
+  // box fraction in [0,1) -> (r-0.5)*2^32 as a wrapping int32
+  return (int)(unsigned int)(long long)llrint((r - 0.5) * kFix);
+}
+
+__device__ inline void write_pack(const DevPtrs& d, const RepConst& c, int prec, int li,
+                                  const double* r, const double* q) {
+  const int ns = c.nsite;
+  if (prec == kF32) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+    uint32_t buf[20];
+    for (int k = 0; k < 20; k++) buf[k] = 0u;
+    buf[0] = (uint32_t)fix_coord(r[0]);
+    buf[1] = (uint32_t)fix_coord(r[1]);
+    buf[2] = (uint32_t)fix_coord(r[2]);
+    for (int k = 0; k < ns; k++) {
+      double o[3];
+      body_to_space(q, c.body[k], o);
+      for (int x = 0; x < 3; x++) buf[3 + 3 * k + x] = __float_as_uint((float)o[x]);
+    }
+    uint4* w4 = reinterpret_cast<uint4*>(w);
+    for (int k = 0; k < c.pack_stride / 4; k++)
+      w4[k] = make_uint4(buf[4 * k], buf[4 * k + 1], buf[4 * k + 2], buf[4 * k + 3]);
+  } else {
+    double* w = reinterpret_cast<double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+    w[0] = r[0]; w[1] = r[1]; w[2] = r[2];
+    for (int k = 0; k < ns; k++) {
+      double o[3];
+      body_to_space(q, c.body[k], o);
+      for (int x = 0; x < 3; x++) w[3 + 3 * k + x] = o[x];
+    }
+  }
+}
+
+__global__ void k_pack(DevPtrs d, int prec) {
+  const Tile t = d.tiles[blockIdx.x];
+  const RepConst& c = d.rc[t.rep];
+  const int i = threadIdx.x;
+  if (i < t.count) {
+    const int li = t.start + i;
+    const int g = c.mol_off + li;
+    double r[3], q[4];
+    for (int x = 0; x < 3; x++) r[x] = d.r[x * d.N + g];
+    for (int x = 0; x < 4; x++) q[x] = d.q[x * d.N + g];
+    write_pack(d, c, prec, li, r, q);
+  }
+  if (i == 0) {
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    d.Lbuild[3 * blockIdx.x] = nan;   // lists must be rebuilt
+  }
+}
+
+// ------------------------------------------------------------------ integrate
+struct StepCoef {
+  double coef_v_a[3], coef_p_a;   // end-of-previous-step kick
+  double coef_v_c[3], coef_p_c;   // this step's kick
+  double coef_xi, cxi1, coef_r[3];
+  double Lb[3];
+};
+
+template <bool MID>
+__global__ void __launch_bounds__(256) k_integrate(DevPtrs d, const RepState* __restrict__ X,
+                                                   RepState* __restrict__ Y, int prec) {
+  __shared__ StepCoef sc;
+  __shared__ double red[8 * 5];
+  const Tile t = d.tiles[blockIdx.x];
+  const RepConst& c = d.rc[t.rep];
+  if (threadIdx.x == 0) {
+    RepState st = X[t.rep];
+    double lj, clmb, wall, vir[3];
+    reduce_part2(d, c, lj, clmb, wall, vir);
+    const double pot = lj + clmb + wall;
+    if (MID) {   // D5 (scalar) + D6 closing the previous step
+      for (int x = 0; x < 3; x++) sc.coef_v_a[x] = st.L[x] * st.s * c.dthalf;
+      sc.coef_p_a = 2.0 * st.s * c.dthalf;
+      d5_scalar(c, st, pot, vir);
+      d6(c, st);
+    }
+    d6(c, st);   // D6 opening this step
+    for (int x = 0; x < 3; x++) sc.coef_v_c[x] = st.L[x] * st.s * c.dthalf;
+    sc.coef_p_c = 2.0 * st.s * c.dthalf;
+    d5_scalar(c, st, pot, vir);
+    d4(c, st);
+    sc.coef_xi = 0.25 / st.s;
+    const double si = 1.0 / st.s;
+    sc.cxi1 = 0.25 * si;
+    for (int x = 0; x < 3; x++) {
+      const double Li = 1.0 / st.L[x];
+      sc.coef_r[x] = Li * Li * si * c.dt;
+    }
+    for (int x = 0; x < 3; x++) sc.Lb[x] = d.Lbuild[3 * blockIdx.x + x];
+    if (blockIdx.x == c.tile_off) Y[t.rep] = st;
+  }
+  __syncthreads();
+  const int i = threadIdx.x;
+  double acc[4] = {0, 0, 0, 0};
+  double disp = 0.0;
+  if (i < t.count) {
+    const int li = t.start + i;
+    const int g = c.mol_off + li;
+    const int N = d.N;
+    double r[3], v[3], q[4], p[4], f[3], n[4];
+    for (int x = 0; x < 3; x++) { r[x] = d.r[x * N + g]; v[x] = d.v[x * N + g]; f[x] = d.f[x * N + g]; }
+    for (int x = 0; x < 4; x++) { q[x] = d.q[x * N + g]; p[x] = d.p[x * N + g]; n[x] = d.n[x * N + g]; }
+    const double m = c.mass;
+    if (MID) kick(v, p, q, f, n, sc.coef_v_a, sc.coef_p_a, m);
+    kick(v, p, q, f, n, sc.coef_v_c, sc.coef_p_c, m);
+    const bool T1 = (c.tconstant == 1);
+    double sPs = 0.0;
+    double xi = rotate(q, p, 3, c.I[2], sc.coef_xi, c.dthalf);
+    if (T1) sPs += 0.5 * xi * xi * c.I[2];
+    xi = rotate(q, p, 2, c.I[1], sc.coef_xi, c.dthalf);
+    if (T1) sPs += 0.5 * xi * xi * c.I[1];
+    for (int x = 0; x < 3; x++) {
+      r[x] += v[x] * sc.coef_r[x];
+      if (r[x] < 0.0) r[x] += 1.0;
+      if (r[x] >= 1.0) r[x] -= 1.0;
+    }
+    xi = rotate(q, p, 1, c.I[0], sc.cxi1, c.dt);
+    if (c.pconstant > 0 || T1)
+      for (int x = 0; x < 3; x++) acc[x] = 2.0 * m * v[x] * v[x];
+    if (T1) sPs += xi * xi * c.I[0];
+    xi = rotate(q, p, 2, c.I[1], sc.coef_xi, c.dthalf);
+    if (T1) sPs += 0.5 * xi * xi * c.I[1];
+    xi = rotate(q, p, 3, c.I[2], sc.coef_xi, c.dthalf);
+    if (T1) sPs += 0.5 * xi * xi * c.I[2];
+    acc[3] = sPs;
+    for (int x = 0; x < 3; x++) { d.r[x * N + g] = r[x]; d.v[x * N + g] = v[x]; }
+    for (int x = 0; x < 4; x++) { d.q[x * N + g] = q[x]; d.p[x * N + g] = p[x]; }
+    write_pack(d, c, prec, li, r, q);
+    // displacement since the last neighbour-list build, in the build box
+    const int4 ref = d.ref_com[g];
+    const int fx = fix_coord(r[0]), fy = fix_coord(r[1]), fz = fix_coord(r[2]);
+    const double dx = (double)(int)(fx - ref.x) * kFixInv * sc.Lb[0];
+    const double dy = (double)(int)(fy - ref.y) * kFixInv * sc.Lb[1];
+    const double dz = (double)(int)(fz - ref.z) * kFixInv * sc.Lb[2];
+    disp = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(disp == disp)) disp = 1e30;   // NaN box: force a rebuild
+  }
+  block_sum<4>(acc, red);
+  disp = block_max(disp, red);
+  if (threadIdx.x == 0) {
+    Part1 pt;
+    pt.sum_Pv[0] = acc[0]; pt.sum_Pv[1] = acc[1]; pt.sum_Pv[2] = acc[2];
+    pt.sum_Ps = acc[3];
+    pt.disp = disp;
+    d.part1[blockIdx.x] = pt;
+  }
+}
+
+// ------------------------------------------------------------------ force
+struct ForceHead {
+  double L[3];
+  int rebuild;
+};
+
+// Neighbour-list rebuild for the molecules of this tile: every molecule of the
+// replica is tested against (rcut+skin), 128 candidates at a time from shared
+// memory (all lanes read the same candidate: a broadcast).
+template <int PREC>
+__device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+                            uint16_t* nb, int tile_size) {
+  __shared__ double4 cand[128];
+  const int i = threadIdx.x;
+  const bool valid = i < t.count;
+  const int li = t.start + i;
+  const double rl = c.rc + c.skin;
+  const double rl2 = rl * rl;
+  int cnt = 0;
+  int ix = 0, iy = 0, iz = 0;
+  double rx = 0, ry = 0, rz = 0;
+  if (valid) {
+    if (PREC == kF32) {
+      const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+      ix = w[0]; iy = w[1]; iz = w[2];
+    } else {
+      const double* w = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+      rx = w[0]; ry = w[1]; rz = w[2];
+    }
+  }
+  for (int base = 0; base < c.nmol; base += 128) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) {
+      const long long off = c.pack_off + (long long)(base + k) * c.pack_stride;
+      if (PREC == kF32) {
+        const int* w = reinterpret_cast<const int*>(d.pack) + off;
+        reinterpret_cast<int4*>(&cand[k])[0] = make_int4(w[0], w[1], w[2], 0);
+      } else {
+        const double* w = reinterpret_cast<const double*>(d.pack) + off;
+        cand[k] = make_double4(w[0], w[1], w[2], 0);
+      }
+    }
+    __syncthreads();
+    if (valid) {
+      const int nk = min(128, c.nmol - base);
+      for (int k = 0; k < nk; k++) {
+        const int j = base + k;
+        double dx, dy, dz;
+        if (PREC == kF32) {
+          const int4 cj = reinterpret_cast<const int4*>(&cand[k])[0];
+          dx = (double)(int)(ix - cj.x) * kFixInv * L[0];
+          dy = (double)(int)(iy - cj.y) * kFixInv * L[1];
+          dz = (double)(int)(iz - cj.z) * kFixInv * L[2];
+        } else {
+          const double4 cj = cand[k];
+          dx = (rx - cj.x) * L[0];
+          dy = (ry - cj.y) * L[1];
+          dz = (rz - cj.z) * L[2];
+          if (dx >= 0.5 * L[0]) dx -= L[0];
+          if (dx < -0.5 * L[0]) dx += L[0];
+          if (dy >= 0.5 * L[1]) dy -= L[1];
+          if (dy < -0.5 * L[1]) dy += L[1];
+          if (dz >= 0.5 * L[2]) dz -= L[2];
+          if (dz < -0.5 * L[2]) dz += L[2];
+        }
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (j != li && r2 < rl2) {
+          if (cnt < c.nbr_cap) nb[(long long)cnt * tile_size] = (uint16_t)j;
+          cnt++;
+        }
+      }
+    }
+  }
+  if (valid) {
+    if (cnt > c.nbr_cap) {
+      atomicOr(d.err, kErrNbrOverflow);
+      atomicMax(&d.status[t.rep], 8);
+      cnt = c.nbr_cap;
+    }
+    d.nbr_cnt[c.mol_off + li] = cnt;
+  }
+}
+
+// Accumulators of one molecule i.
+struct IAcc {
+  double fs[kMaxSites][3];   // site forces (switched pair terms + wall on site 0)
+  double fc[3];              // switching correction -E dS/dr r^ (acts on the molecule only)
+  double vir[3], lj, clmb;
+  long long npair;
+};
+
+// FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU),
+// partial sums in FP32 over at most 16 neighbours, then FP64 accumulation.
+template <int S, int C0>
+__device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+                              const uint16_t* nb, int cnt, IAcc& a) {
+  constexpr int STRIDE = ((3 + 3 * S) + 3) / 4 * 4;
+  const int li = t.start + threadIdx.x;
+  const uint32_t* base = reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off;
+  uint32_t wi[STRIDE];
+  {
+    const uint4* p4 = reinterpret_cast<const uint4*>(base + (long long)li * STRIDE);
+#pragma unroll
+    for (int k = 0; k < STRIDE / 4; k++) {
+      const uint4 u = __ldg(p4 + k);
+      wi[4 * k] = u.x; wi[4 * k + 1] = u.y; wi[4 * k + 2] = u.z; wi[4 * k + 3] = u.w;
+    }
+  }
+  const int xi = (int)wi[0], yi = (int)wi[1], zi = (int)wi[2];
+  float si[S][3];
+#pragma unroll
+  for (int k = 0; k < S; k++)
+#pragma unroll
+    for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
+  float qq[S][S];
+#pragma unroll
+  for (int k = 0; k < S; k++)
+#pragma unroll
+    for (int l = 0; l < S; l++) qq[k][l] = (float)c.qq[k][l];
+  const float Lsx = (float)(L[0] * kFixInv), Lsy = (float)(L[1] * kFixInv),
+              Lsz = (float)(L[2] * kFixInv);
+  const float rc = (float)c.rc, rs = (float)c.rs, rc2 = (float)(c.rc * c.rc);
+  const float coef = (float)c.coef_sw;
+  const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
+
+  float fs[S][3], fc[3], fv[3], flj, fcl;
+  auto zero = [&]() {
+#pragma unroll
+    for (int k = 0; k < S; k++) fs[k][0] = fs[k][1] = fs[k][2] = 0.f;
+    fc[0] = fc[1] = fc[2] = 0.f;
+    fv[0] = fv[1] = fv[2] = 0.f;
+    flj = fcl = 0.f;
+  };
+  auto flush = [&]() {
+#pragma unroll
+    for (int k = 0; k < S; k++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) a.fs[k][x] += (double)fs[k][x];
+#pragma unroll
+    for (int x = 0; x < 3; x++) { a.fc[x] += (double)fc[x]; a.vir[x] += (double)fv[x]; }
+    a.lj += (double)flj;
+    a.clmb += (double)fcl;
+  };
+  zero();
+  long long np = 0;
+  for (int k = 0; k < cnt; k++) {
+    const int j = nb[(long long)k * blockDim.x];
+    uint32_t wj[STRIDE];
+    const uint4* p4 = reinterpret_cast<const uint4*>(base + (long long)j * STRIDE);
+#pragma unroll
+    for (int m = 0; m < STRIDE / 4; m++) {
+      const uint4 u = __ldg(p4 + m);
+      wj[4 * m] = u.x; wj[4 * m + 1] = u.y; wj[4 * m + 2] = u.z; wj[4 * m + 3] = u.w;
+    }
+    const float dx = (float)(int)(xi - (int)wj[0]) * Lsx;
+    const float dy = (float)(int)(yi - (int)wj[1]) * Lsy;
+    const float dz = (float)(int)(zi - (int)wj[2]) * Lsz;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= rc2) {
+      np++;
+      const float rinv = rsqrtf(r2);
+      const float r = r2 * rinv;
+      float sw = 1.f, dsw = 0.f;
+      if (r > rs) {
+        const float r01c = r - rc, r01l = r - rs;
+        sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
+        dsw = coef * 30.f * r01c * r01c * r01l * r01l;
+      }
+      float sj[S][3];
+#pragma unroll
+      for (int l = 0; l < S; l++)
+#pragma unroll
+        for (int x = 0; x < 3; x++) sj[l][x] = __uint_as_float(wj[3 + 3 * l + x]);
+      float elj = 0.f, ecl = 0.f;
+      float fpx = 0.f, fpy = 0.f, fpz = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < S; kk++) {
+        if (kk != 0 && kk < C0) continue;
+        const float ax = dx + si[kk][0], ay = dy + si[kk][1], az = dz + si[kk][2];
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+        for (int l = 0; l < S; l++) {
+          const bool lj_pair = (kk == 0 && l == 0);
+          const bool cl_pair = (kk >= C0 && l >= C0);
+          if (!lj_pair && !cl_pair) continue;
+          const float x = ax - sj[l][0], y = ay - sj[l][1], z = az - sj[l][2];
+          const float rr = x * x + y * y + z * z;
+          const float ri = rsqrtf(rr);
+          const float ri2 = ri * ri;
+          float ftmp = 0.f;
+          if (lj_pair) {
+            float s6 = sgm2 * ri2;
+            s6 = s6 * s6 * s6;
+            elj += eps4 * s6 * (s6 - 1.f);
+            ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
+          }
+          if (cl_pair) {
+            const float e = qq[kk][l] * ri;
+            ecl += e;
+            ftmp += e * ri2;
+          }
+          ftmp *= sw;
+          tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
+        }
+        fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
+        fpx += tx; fpy += ty; fpz += tz;
+      }
+      const float e = elj + ecl;
+      const float g = dsw * rinv * e;
+      const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
+      fc[0] += cx; fc[1] += cy; fc[2] += cz;
+      fv[0] += (fpx + cx) * dx;
+      fv[1] += (fpy + cy) * dy;
+      fv[2] += (fpz + cz) * dz;
+      flj += sw * elj;
+      fcl += sw * ecl;
+    }
+    if ((k & 15) == 15) { flush(); zero(); }
+  }
+  flush();
+  a.npair += np;
+}
+
+// FP64 pair loop: the reference's generic Switching (src/force_calculator.cxx:691-779)
+// arithmetic for molecule i, over its neighbour list.
+template <int S, int C0>
+__device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+                              const uint16_t* nb, int cnt, IAcc& a) {
+  constexpr int STRIDE = ((3 + 3 * S) + 1) / 2 * 2;
+  const int li = t.start + threadIdx.x;
+  const double* base = reinterpret_cast<const double*>(d.pack) + c.pack_off;
+  double wi[STRIDE];
+#pragma unroll
+  for (int k = 0; k < STRIDE; k++) wi[k] = base[(long long)li * STRIDE + k];
+  const double rc = c.rc, rl = c.rs, coef = c.coef_sw, rc2 = c.rc * c.rc;
+  for (int k = 0; k < cnt; k++) {
+    const int j = nb[(long long)k * blockDim.x];
+    const double* wj = base + (long long)j * STRIDE;
+    double gr[3];
+    for (int x = 0; x < 3; x++) {
+      gr[x] = (wi[x] - wj[x]) * L[x];
+      if (gr[x] >= 0.5 * L[x]) gr[x] -= L[x];
+      if (gr[x] < -0.5 * L[x]) gr[x] += L[x];
+    }
+    const double r02 = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+    if (r02 > rc2) continue;
+    a.npair++;
+    const double r01 = sqrt(r02);
+    double sw = 1.0, dsw = 0.0;
+    if (r01 > rl) {
+      const double r01c = r01 - rc, r01l = r01 - rl;
+      sw = coef * r01c * r01c * r01c * (10.0 * r01l * r01l - 5.0 * r01l * r01c + r01c * r01c);
+      dsw = coef * 30.0 * r01c * r01c * r01l * r01l;
+    }
+    double dswr[3];
+    for (int x = 0; x < 3; x++) dswr[x] = gr[x] * (dsw / r01);
+#pragma unroll
+    for (int kk = 0; kk < S; kk++) {
+      if (kk != 0 && kk < C0) continue;
+      double e = 0.0, f[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int l = 0; l < S; l++) {
+        const bool lj_pair = (kk == 0 && l == 0);
+        const bool cl_pair = (kk >= C0 && l >= C0);
+        if (!lj_pair && !cl_pair) continue;
+        double rv[3];
+        for (int x = 0; x < 3; x++) rv[x] = gr[x] + wi[3 + 3 * kk + x] - wj[3 + 3 * l + x];
+        const double rr = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+        const double r02i = 1.0 / rr;
+        const double r01i = sqrt(r02i);
+        const double qq = cl_pair ? c.qq[kk][l] : 0.0;
+        double elj = 0.0, flj = 0.0;
+        if (lj_pair) {
+          double rs06i = c.sgm2 * r02i;
+          rs06i = rs06i * rs06i * rs06i;
+          elj = 4.0 * c.eps * rs06i * (rs06i - 1.0);
+          flj = 48.0 * c.eps * rs06i * (rs06i - 0.5) * r02i;
+        }
+        const double ecl = qq * r01i;
+        a.lj += sw * elj;
+        a.clmb += sw * ecl;
+        const double ftmp = (flj + qq * r01i * r02i) * sw;
+        e += elj + ecl;
+        for (int x = 0; x < 3; x++) {
+          f[x] += rv[x] * ftmp;
+          a.fs[kk][x] += rv[x] * ftmp;
+        }
+      }
+      for (int x = 0; x < 3; x++) {
+        const double cx = -dswr[x] * e;
+        a.fc[x] += cx;
+        a.vir[x] += (f[x] + cx) * gr[x];
+      }
+    }
+  }
+}
+
+template <int S, int C0, int PREC>
+__device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+                           bool rebuild, int tile_size) {
+  __shared__ double red[8 * 8];
+  const int i = threadIdx.x;
+  const bool valid = i < t.count;
+  const int li = t.start + i;
+  const int g = c.mol_off + li;
+  uint16_t* nb = d.nbr + c.nbr_off + (long long)(blockIdx.x - c.tile_off) * c.nbr_cap * tile_size + i;
+  if (rebuild) {
+    build_lists<PREC>(d, c, t, L, nb, tile_size);
+    __syncthreads();
+    if (valid) {
+      const int* w;
+      int4 rc4;
+      if (PREC == kF32) {
+        w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+        rc4 = make_int4(w[0], w[1], w[2], 0);
+      } else {
+        const double* wd = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+        rc4 = make_int4(fix_coord(wd[0]), fix_coord(wd[1]), fix_coord(wd[2]), 0);
+      }
+      d.ref_com[g] = rc4;
+    }
+    if (i == 0)
+      for (int x = 0; x < 3; x++) d.Lbuild[3 * blockIdx.x + x] = L[x];
+  }
+  IAcc a;
+#pragma unroll
+  for (int k = 0; k < kMaxSites; k++) a.fs[k][0] = a.fs[k][1] = a.fs[k][2] = 0.0;
+  a.fc[0] = a.fc[1] = a.fc[2] = 0.0;
+  a.vir[0] = a.vir[1] = a.vir[2] = 0.0;
+  a.lj = a.clmb = 0.0;
+  a.npair = 0;
+  double wall_e = 0.0;
+  if (valid) {
+    const int cnt = d.nbr_cnt[g];
+    if (PREC == kF32)
+      pair_loop_f32<S, C0>(d, c, t, L, nb, cnt, a);
+    else
+      pair_loop_f64<S, C0>(d, c, t, L, nb, cnt, a);
+    const int N = d.N;
+    double q[4], r[3];
+    for (int x = 0; x < 4; x++) q[x] = d.q[x * N + g];
+    for (int x = 0; x < 3; x++) r[x] = d.r[x * N + g];
+    // wall on the oxygen site (ForceCalculator::Confined, src/force_calculator.cxx:1527-1566;
+    // slit: src/remdgpu.cu:1708-1720)
+    if (c.confined > 0) {
+      double o[3];
+      body_to_space(q, c.body[0], o);
+      const double2* fw = reinterpret_cast<const double2*>(d.wall) + c.wall_off;
+      const double dr = c.wall_dr;
+      if (c.confined == 1) {
+        const double x = r[0] * L[0] + o[0] - L[0] * 0.5;
+        const double y = r[1] * L[1] + o[1] - L[1] * 0.5;
+        const double r01 = sqrt(x * x + y * y);
+        int idx = (r01 >= 0.0) ? (int)fmin(r01 / dr, (double)(c.nfwall - 2)) : 0;   // NaN -> 0
+        const double2 w0 = fw[idx], w1 = fw[idx + 1];
+        const double f = (w1.x - w0.x) / dr * (r01 - dr * idx) + w0.x;
+        const double e = (w1.y - w0.y) / dr * (r01 - dr * idx) + w0.y;
+        a.fs[0][0] += f * x;
+        a.fs[0][1] += f * y;
+        wall_e = e;
+      } else {
+        const double z = r[2] * L[2] + o[2] - 0.5 * L[2];
+        const double za = fabs(z);
+        const double dir = (za != 0.0) ? z / za : 1.0;
+        int idx = (za >= 0.0) ? (int)fmin(za / dr, (double)(c.nfwall - 2)) : 0;     // NaN -> 0
+        const double2 w0 = fw[idx], w1 = fw[idx + 1];
+        const double f = (w1.x - w0.x) / dr * (za - dr * idx) + w0.x;
+        const double e = (w1.y - w0.y) / dr * (za - dr * idx) + w0.y;
+        a.fs[0][2] += f * dir;
+        wall_e = e;
+      }
+    }
+    // A2M: molecular force and body torque (src/molecules.cxx:447-475)
+    double F[3] = {a.fc[0], a.fc[1], a.fc[2]};
+    double nq[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < S; k++) {
+      for (int x = 0; x < 3; x++) F[x] += a.fs[k][x];
+      double fb[3];
+      space_to_body(q, a.fs[k], fb);
+      const double* b = c.body[k];
+      nq[0] += b[0] * fb[0] + b[1] * fb[1] + b[2] * fb[2];
+      nq[1] += b[1] * fb[2] - b[2] * fb[1];
+      nq[2] += b[2] * fb[0] - b[0] * fb[2];
+      nq[3] += b[0] * fb[1] - b[1] * fb[0];
+    }
+    for (int x = 0; x < 3; x++) d.f[x * N + g] = F[x];
+    for (int x = 0; x < 4; x++) d.n[x * N + g] = nq[x];
+  }
+  double s6[7] = {a.lj, a.clmb, wall_e, a.vir[0], a.vir[1], a.vir[2], (double)a.npair};
+  block_sum<7>(s6, red);
+  if (threadIdx.x == 0) {
+    Part2 p;
+    p.lj = s6[0]; p.clmb = s6[1]; p.wall = s6[2];
+    p.vir[0] = s6[3]; p.vir[1] = s6[4]; p.vir[2] = s6[5];
+    p.npairs = (long long)llrint(s6[6]);
+    p.pad = 0.0;
+    d.part2[blockIdx.x] = p;
+  }
+}
+
+template <int PREC, bool FORCE_ONLY>
+__global__ void __launch_bounds__(256) k_force(DevPtrs d, const RepState* __restrict__ Yin,
+                                               RepState* __restrict__ Xout, int tile_size) {
+  __shared__ ForceHead h;
+  const Tile t = d.tiles[blockIdx.x];
+  const RepConst& c = d.rc[t.rep];
+  if (threadIdx.x == 0) {
+    RepState st = Yin[t.rep];
+    if (!FORCE_ONLY) {
+      double sPv[3] = {0, 0, 0}, sPs = 0.0, disp = 0.0;
+      for (int k = c.tile_off; k < c.tile_off + c.ntile; k++) {
+        const Part1 p = d.part1[k];
+        sPv[0] += p.sum_Pv[0]; sPv[1] += p.sum_Pv[1]; sPv[2] += p.sum_Pv[2];
+        sPs += p.sum_Ps;
+        disp = fmax(disp, p.disp);
+      }
+      pspv(c, st, sPv, sPs);
+      d4(c, st);
+      if (blockIdx.x == c.tile_off) Xout[t.rep] = st;
+      // list validity: pairs now within rc were within rc+skin at the build if
+      // 2*max|displacement| + rc*(max_d Lbuild_d/L_d - 1) <= skin
+      const double lb0 = d.Lbuild[3 * blockIdx.x], lb1 = d.Lbuild[3 * blockIdx.x + 1],
+                   lb2 = d.Lbuild[3 * blockIdx.x + 2];
+      int rb = !(lb0 == lb0);
+      if (!rb) {
+        const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
+        rb = (2.0 * disp + c.rc * (lam - 1.0) > c.skin);
+      }
+      h.rebuild = rb;
+    } else {
+      h.rebuild = 1;
+    }
+    for (int x = 0; x < 3; x++) h.L[x] = st.L[x];
+  }
+  __syncthreads();
+  const double L[3] = {h.L[0], h.L[1], h.L[2]};
+  const bool rb = h.rebuild != 0;
+  if (c.nsite == 3)
+    force_tile<3, 0, PREC>(d, c, t, L, rb, tile_size);
+  else if (c.nsite == 4)
+    force_tile<4, 1, PREC>(d, c, t, L, rb, tile_size);
+  else
+    force_tile<5, 1, PREC>(d, c, t, L, rb, tile_size);
+}
+
+// ------------------------------------------------------------------ per-replica kernels
+constexpr int kRepThreads = 256;
+
+__device__ inline double barostat_energy(const RepConst& c, const RepState& st) {
+  // Molecules::BarostatEnergy (src/molecules.cxx:663-678); slit src/remdgpu.cu:2803-2809
+  if (c.pconstant > 0) {
+    if (c.confined == 0)
+      return 0.5 * (st.Pv[0] * st.Pv[0] + st.Pv[1] * st.Pv[1] + st.Pv[2] * st.Pv[2]) / c.W +
+             st.P * st.L[0] * st.L[1] * st.L[2];
+    if (c.confined == 1) return 0.5 * st.Pv[2] * st.Pv[2] / c.W + st.P * volume(c, st);
+    return (st.Pv[0] * st.Pv[0] + st.Pv[1] * st.Pv[1]) * (0.5 / c.W) + st.P * volume(c, st);
+  }
+  return 0.0;
+}
+
+// Molecules::CalcProperties (src/molecules.cxx:702-734) from the reduced kinetic
+// sums; writes the REMDGPU::GetAverages fields (T and pressures reduced).
+__device__ inline double calc_properties(const DevPtrs& d, const RepConst& c, const RepState& st,
+                                         const double* tra3raw, double rot, double* avg) {
+  double lj, clmb, wall, vir[3];
+  reduce_part2(d, c, lj, clmb, wall, vir);
+  const double pot = lj + clmb + wall;
+  double tmp[3];
+  for (int x = 0; x < 3; x++) {
+    const double cf = 1.0 / (st.L[x] * st.s);
+    tmp[x] = tra3raw[x] * (cf * cf * 0.5);
+  }
+  const double tra = tmp[0] + tmp[1] + tmp[2];
+  const double kin = tra + rot;
+  const double tsm = 0.5 * st.Ps * st.Ps / c.Q;
+  const double tsp = st.gkT * log(st.s);
+  double tot = pot + kin;
+  if (c.tconstant == 1) tot += tsm + tsp;
+  if (c.pconstant > 0) tot += barostat_energy(c, st);
+  const double V = volume(c, st);
+  if (avg) {
+    avg[0] = lj; avg[1] = clmb; avg[2] = wall; avg[3] = V;
+    avg[4] = tra; avg[5] = rot; avg[6] = kin / (3.0 * c.nmol);
+    avg[8] = (tmp[0] * 2.0 + vir[0]) / V;
+    avg[9] = (tmp[1] * 2.0 + vir[1]) / V;
+    avg[10] = (tmp[2] * 2.0 + vir[2]) / V;
+    avg[7] = ((tmp[0] * 2.0 + vir[0]) + (tmp[1] * 2.0 + vir[1]) + (tmp[2] * 2.0 + vir[2])) / (3. * V);
+    avg[11] = tot; avg[12] = tot - st.H0;
+    avg[13] = st.s; avg[14] = st.Ps;
+    avg[15] = st.Pv[0]; avg[16] = st.Pv[1]; avg[17] = st.Pv[2]; avg[18] = 0.0;
+  }
+  return tot;
+}
+
+__device__ inline void kinetic_sums(const DevPtrs& d, const RepConst& c, double s, double* acc) {
+  const int N = d.N;
+  acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    double q[4], p[4];
+    for (int x = 0; x < 4; x++) { q[x] = d.q[x * N + g]; p[x] = d.p[x * N + g]; }
+    for (int x = 0; x < 3; x++) {
+      const double v = d.v[x * N + g];
+      acc[x] += (v * v) * c.mass;
+    }
+    acc[3] += rot_energy(q, p, c.I, s);
+  }
+}
+
+__device__ inline void finish_replica(const DevPtrs& d, const RepConst& c, int rep, const RepState& st) {
+  double* avg = d.avg + (long long)rep * kNumAvg;
+  bool ok = true;
+  for (int k = 0; k < kNumAvg; k++) ok = ok && isfinite(avg[k]);
+  if (!ok) {
+    atomicOr(d.err, kErrNonFinite);
+    atomicMax(&d.status[rep], 4);
+  }
+}
+
+__global__ void __launch_bounds__(kRepThreads) k_replica_end(DevPtrs d, RepState* X) {
+  __shared__ RepState st;
+  __shared__ double cv[4];
+  __shared__ double red[8 * 4];
+  const int rep = blockIdx.x;
+  const RepConst& c = d.rc[rep];
+  if (threadIdx.x == 0) {
+    RepState s = X[rep];
+    double lj, clmb, wall, vir[3];
+    reduce_part2(d, c, lj, clmb, wall, vir);
+    for (int x = 0; x < 3; x++) cv[x] = s.L[x] * s.s * c.dthalf;
+    cv[3] = 2.0 * s.s * c.dthalf;
+    d5_scalar(c, s, lj + clmb + wall, vir);
+    d6(c, s);
+    st = s;
+  }
+  __syncthreads();
+  const int N = d.N;
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    double v[3], p[4], q[4], f[3], n[4];
+    for (int x = 0; x < 3; x++) { v[x] = d.v[x * N + g]; f[x] = d.f[x * N + g]; }
+    for (int x = 0; x < 4; x++) { q[x] = d.q[x * N + g]; p[x] = d.p[x * N + g]; n[x] = d.n[x * N + g]; }
+    kick(v, p, q, f, n, cv, cv[3], c.mass);
+    for (int x = 0; x < 3; x++) d.v[x * N + g] = v[x];
+    for (int x = 0; x < 4; x++) d.p[x * N + g] = p[x];
+  }
+  __syncthreads();
+  double acc[4];
+  kinetic_sums(d, c, st.s, acc);
+  block_sum<4>(acc, red);
+  if (threadIdx.x == 0) {
+    calc_properties(d, c, st, acc, acc[3], d.avg + (long long)rep * kNumAvg);
+    X[rep] = st;
+    finish_replica(d, c, rep, st);
+  }
+}
+
+// Initial properties after the first force call: gkT, CalcProperties, H0 = tot
+// (Molecules::InitializeProperty, src/molecules.h:260-270).
+__global__ void __launch_bounds__(kRepThreads) k_replica_props(DevPtrs d, RepState* X) {
+  __shared__ double red[8 * 4];
+  const int rep = blockIdx.x;
+  const RepConst& c = d.rc[rep];
+  RepState st = X[rep];
+  double acc[4];
+  kinetic_sums(d, c, st.s, acc);
+  block_sum<4>(acc, red);
+  if (threadIdx.x == 0) {
+    st.gkT = 6.0 * (double)c.nmol * st.T;
+    double* avg = d.avg + (long long)rep * kNumAvg;
+    st.H0 = calc_properties(d, c, st, acc, acc[3], avg);
+    avg[12] = 0.0;
+    X[rep] = st;
+  }
+}
+
+// The exchange tail for a replica whose condition changed (src/remd.cxx:526-536):
+// ChangeTemperature (src/molecules.h:333-353), KillMomentum (+ the tube's angular
+// momentum, src/molecules.cxx:168-210), SetPressure, CalcProperties, UpdateHamiltonian.
+__global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepState* X) {
+  __shared__ RepState st;
+  __shared__ double sh[4];
+  __shared__ double red[8 * 4];
+  const int rep = blockIdx.x;
+  const RepConst& c = d.rc[rep];
+  const double Tn = d.newT[rep], Pn = d.newP[rep];
+  {
+    const RepState s0 = X[rep];
+    if (Tn == s0.T && Pn == s0.P) return;   // uniform over the block
+  }
+  if (threadIdx.x == 0) {
+    RepState s = X[rep];
+    const double coef = sqrt(Tn / s.T);
+    sh[0] = coef / s.s;
+    s.Ps *= coef;
+    if (c.pconstant == 1) s.Pv[0] *= coef * s.s;
+    if (c.pconstant == 2) s.Pv[2] *= coef * s.s;
+    if (c.pconstant == 3) { s.Pv[0] *= coef * s.s; s.Pv[1] *= coef * s.s; }
+    s.T = Tn;
+    s.gkT = 6.0 * (double)c.nmol * s.T;
+    s.s = 1.0;
+    st = s;
+  }
+  __syncthreads();
+  const int N = d.N;
+  const double sc = sh[0];
+  double acc[4] = {0, 0, 0, 0};
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    for (int x = 0; x < 3; x++) {
+      const double v = d.v[x * N + g] * sc;
+      d.v[x * N + g] = v;
+      acc[x] += v * c.mass;
+    }
+    for (int x = 0; x < 4; x++) d.p[x * N + g] *= sc;
+    acc[3] += c.mass;
+  }
+  block_sum<4>(acc, red);
+  const double mom[3] = {acc[0] / acc[3], acc[1] / acc[3], acc[2] / acc[3]};
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    if (c.confined == 1) {
+      d.v[2 * N + g] -= mom[2];
+    } else if (c.confined == 2) {
+      d.v[g] -= mom[0];
+      d.v[N + g] -= mom[1];
+    } else {
+      for (int x = 0; x < 3; x++) d.v[x * N + g] -= mom[x];
+    }
+  }
+  __syncthreads();
+  if (c.confined == 1) {   // KillAngularMomentumInTube
+    double am[4] = {0, 0, 0, 0};
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+      const int g = c.mol_off + li;
+      double r[3], v[3];
+      for (int x = 0; x < 3; x++) {
+        r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+        v[x] = d.v[x * N + g] / (st.L[x] * st.s);
+      }
+      am[0] += c.mass * (r[0] * v[1] - r[1] * v[0]);
+      am[1] += c.mass;
+    }
+    block_sum<4>(am, red);
+    const double lz = am[0] / am[1];
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+      const int g = c.mol_off + li;
+      double r[3];
+      for (int x = 0; x < 3; x++) r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+      const double r02 = r[0] * r[0] + r[1] * r[1];
+      if (r02 > 1.0) {
+        d.v[g] += lz * r[1] / r02 * st.L[0] * st.s;
+        d.v[N + g] -= lz * r[0] / r02 * st.L[1] * st.s;
+      }
+    }
+    __syncthreads();
+  }
+  double kacc[4];
+  kinetic_sums(d, c, st.s, kacc);
+  block_sum<4>(kacc, red);
+  if (threadIdx.x == 0) {
+    RepState s = st;
+    s.P = Pn;
+    s.H0 = calc_properties(d, c, s, kacc, kacc[3], nullptr);
+    X[rep] = s;
+  }
+}
+
+// ------------------------------------------------------------------ exchange
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): a counter-based generator.
+__device__ inline uint4 philox4x32(uint4 ctr, uint2 key) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  for (int i = 0; i < 10; i++) {
+    const uint32_t hi0 = __umulhi(M0, ctr.x), lo0 = M0 * ctr.x;
+    const uint32_t hi1 = __umulhi(M1, ctr.z), lo1 = M1 * ctr.z;
+    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
+    key.x += W0;
+    key.y += W1;
+  }
+  return ctr;
+}
+
+__device__ inline double philox_uniform(unsigned long long seed, long step, int ens, int pair) {
+  const uint4 r = philox4x32(make_uint4((uint32_t)pair, (uint32_t)ens, (uint32_t)step,
+                                        (uint32_t)((unsigned long long)step >> 32)),
+                             make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  const unsigned long long b = ((unsigned long long)r.x << 32 | r.y) >> 11;
+  return (double)b * (1.0 / 9007199254740992.0);
+}
+
+// REMD::ReplicaExchange + ExchangeList (src/remd.cxx:467-538, src/remdinfo.cxx:54-125),
+// one thread per ensemble; pot/vol from the averages of the last interval.
+__global__ void k_exchange(DevPtrs d, const int* grid, const int* rep_off, const int* u_off,
+                           int nens, long step, const double* u, unsigned long long seed,
+                           int* index, double* T, double* P) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nens) return;
+  const int nt = grid[2 * e], np = grid[2 * e + 1];
+  const int off = rep_off[e];
+  const int pcon = d.rc[off].pconstant;
+  const int ec = (int)(step % 4);
+  int* idx = index + off;
+  double* Te = T + off;
+  double* Pe = P + off;
+  auto pot_of = [&](int r) {
+    const double* a = d.avg + (long long)(off + r) * kNumAvg;
+    return a[0] + a[1] + a[2];
+  };
+  auto vol_of = [&](int r) { return d.avg[(long long)(off + r) * kNumAvg + 3]; };
+  int pair = 0;
+  auto trial = [&](int a, int b) {
+    const int i1 = idx[a], i2 = idx[b];
+    const double b1 = 1. / Te[i1], b2 = 1. / Te[i2];
+    double delta = (b2 - b1) * (pot_of(i1) - pot_of(i2));
+    if (pcon > 0) delta += (b2 * Pe[i2] - b1 * Pe[i1]) * (vol_of(i1) - vol_of(i2));
+    const double uu = u ? u[u_off[e] + pair] : philox_uniform(seed, step, e, pair);
+    pair++;
+    if (exp(-delta) > uu) {
+      double t = Te[idx[a]]; Te[idx[a]] = Te[idx[b]]; Te[idx[b]] = t;
+      t = Pe[idx[a]]; Pe[idx[a]] = Pe[idx[b]]; Pe[idx[b]] = t;
+      const int ti = idx[a]; idx[a] = idx[b]; idx[b] = ti;
+    }
+  };
+  if (ec == 0) {
+    for (int j = 0; j < np; ++j)
+      for (int i = 0; i < nt / 2; ++i) trial(2 * i + j * nt, 2 * i + 1 + j * nt);
+  } else if (ec == 1) {
+    for (int j = 0; j < np / 2; ++j)
+      for (int i = 0; i < nt; ++i) trial(i + 2 * j * nt, i + (2 * j + 1) * nt);
+  } else if (ec == 2) {
+    for (int j = 0; j < np; ++j)
+      for (int i = 0; i < nt / 2 - (nt + 1) % 2; ++i) trial(2 * i + j * nt + 1, 2 * i + 1 + j * nt + 1);
+  } else {
+    for (int j = 0; j < np / 2 - (np + 1) % 2; ++j)
+      for (int i = 0; i < nt; ++i) trial(i + (2 * j + 1) * nt, i + (2 * j + 2) * nt);
+  }
+}
+
+// ------------------------------------------------------------------ FP32 peak probe
+// Eight independent FMA chains per thread, register resident: measures the
+// FP32 pipe's FMA throughput (the force kernel's roofline denominator).
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a, float b) {
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+  float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+    }
+  }
+  const float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 12345.678f) out[blockIdx.x] = s;   // keeps the chains live
+}
+
+int measure_fp32_fma(int device, double* ms, long long* flops) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 6;
+  const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 4096;
+  float* out = nullptr;
+  if (cudaMalloc(&out, blocks * sizeof(float)) != cudaSuccess) return 2;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fma_peak<<<blocks, threads>>>(out, 64, 0.999f, 1e-3f);   // warm-up
+  float best = 1e30f;
+  for (int rep = 0; rep < 5; rep++) {
+    cudaEventRecord(e0);
+    k_fma_peak<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    best = fminf(best, t);
+  }
+  const cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (err != cudaSuccess) return 6;
+  *ms = best;
+  *flops = (long long)blocks * threads * iters * 16LL * 8LL * 2LL;
+  return 0;
+}
+
+// ------------------------------------------------------------------ launchers
+void launch_pack(const DevPtrs& d, int prec, int tile, cudaStream_t s) {
+  k_pack<<<d.ntiles, tile, 0, s>>>(d, prec);
+}
+void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, bool mid, int tile,
+                           int prec, cudaStream_t s) {
+  if (mid)
+    k_integrate<true><<<d.ntiles, tile, 0, s>>>(d, X, Y, prec);
+  else
+    k_integrate<false><<<d.ntiles, tile, 0, s>>>(d, X, Y, prec);
+}
+void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
+                  int tile, cudaStream_t s) {
+  if (prec == kF32) {
+    if (force_only) k_force<kF32, true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    else k_force<kF32, false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+  } else {
+    if (force_only) k_force<kF64, true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    else k_force<kF64, false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+  }
+}
+void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s) {
+  k_replica_start<<<d.nrep, kRepThreads, 0, s>>>(d, X);
+}
+void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s) {
+  k_replica_end<<<d.nrep, kRepThreads, 0, s>>>(d, X);
+}
+void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s) {
+  k_replica_props<<<d.nrep, kRepThreads, 0, s>>>(d, X);
+}
+void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
+                       int nens, long step, const double* u, unsigned long long seed, int* index,
+                       double* T, double* P, cudaStream_t s) {
+  k_exchange<<<(nens + 63) / 64, 64, 0, s>>>(d, grid, rep_off, u_off, nens, step, u, seed, index, T, P);
+}
+
+}  // namespace remd

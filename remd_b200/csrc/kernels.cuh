@@ -1,0 +1,39 @@
+// kernels.cuh -- the engine's CUDA kernels (sm_100a).
+//
+// One MD step of every replica of every ensemble is two launches over the same
+// tile grid (a tile = `blockDim.x` consecutive molecules of one replica):
+//
+//   k_integrate  [end of the previous step: D5 kick, D5/D6 scalars]
+//                D6, D5, D4, D3 D2 D1 D2 D3 (src/integrator.cxx:646-673),
+//                then the force record of every molecule (fixed-point centre of
+//                mass + rotated site offsets) and the partial sums PsPv needs;
+//   k_force      PsPv + D4 (scalar chain), a neighbour-list rebuild when the
+//                skin criterion fails, the switched LJ + Coulomb pair loop,
+//                the wall, and the site -> molecule torque (A2M).
+//
+// An interval is k_replica_start (exchange tail), interval x (k_integrate,
+// k_force), k_replica_end (last D5/D6 + CalcProperties -> Average), captured
+// once as a CUDA graph.
+#pragma once
+#include "engine_types.cuh"
+
+namespace remd {
+
+enum Prec : int { kF32 = 0, kF64 = 1 };
+
+// host-side launchers (kernels.cu)
+void launch_pack(const DevPtrs& d, int prec, int tile, cudaStream_t s);
+void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, bool mid, int tile,
+                           int prec, cudaStream_t s);
+void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
+                  int tile, cudaStream_t s);
+void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s);
+void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s);
+void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);
+void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
+                       int nens, long step, const double* u, unsigned long long seed, int* index,
+                       double* T, double* P, cudaStream_t s);
+int pack_stride(int nsite, int prec);
+int measure_fp32_fma(int device, double* ms, long long* flops);
+
+}  // namespace remd

@@ -1,0 +1,293 @@
+"""Python mirror of the reference's REMDGPU call surface (src/remdgpu.h:92-238)
+over the C-ABI of libremd_b200.so (include/remd_b200.h).
+
+    eng = REMDGPU(ensembles, precision="fp32")
+    eng.ExecuteSteps(T, P)          # one interval for every replica
+    avg = eng.GetAverages(rep)      # the 19 Average fields
+    st  = eng.ConvertVariablesToHost(rep)
+
+The compute path is the CUDA library; there is no CPU fallback.  If the library
+is missing it is built with nvcc (remd_b200/csrc/Makefile); if that fails, or
+no GPU is visible, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from .inputs import ReplicaState
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libremd_b200.so")
+NUM_AVG = 19
+AVG_NAMES = ["LJ", "CLMB", "WALL", "VOL", "TRA", "ROT", "T", "P", "Px", "Py", "Pz",
+             "TOT", "DRF", "TSTs", "TSTv", "BSTx", "BSTy", "BSTz", "DUMMY"]
+STATUS = {0: "OK", 1: "INVALID", 2: "OOM", 3: "TIMEOUT", 4: "NONFINITE", 5: "CANCELLED",
+          6: "CUDA", 7: "IO", 8: "NEIGHBOR_OVERFLOW", 9: "NO_DEVICE"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class RemdError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"remd status {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [("nmol", C.c_int), ("nsite", C.c_int), ("site_r", (C.c_double * 3) * 5),
+                ("site_mass", C.c_double * 5), ("site_sigma", C.c_double * 5),
+                ("site_eps", C.c_double * 5), ("site_charge", C.c_double * 5),
+                ("tconstant", C.c_int), ("pconstant", C.c_int), ("confined", C.c_int),
+                ("dt_fs", C.c_double), ("rcut", C.c_double), ("rswitch", C.c_double),
+                ("nfwall", C.c_int), ("wall_length", C.c_double), ("sgm_wall", C.c_double),
+                ("eps_wall", C.c_double), ("rho_wall", C.c_double), ("interval", C.c_int)]
+
+
+class ReplicaInit(C.Structure):
+    _fields_ = [("r", _dp), ("v", _dp), ("q", _dp), ("p", _dp), ("mass", _dp),
+                ("inertia", _dp), ("s", C.c_double), ("Ps", C.c_double), ("Q", C.c_double),
+                ("Pv", C.c_double * 3), ("W", C.c_double), ("L", C.c_double * 3),
+                ("T", C.c_double), ("P", C.c_double)]
+
+
+class StateView(C.Structure):
+    _fields_ = [("r", _dp), ("v", _dp), ("q", _dp), ("p", _dp), ("f", _dp), ("n", _dp),
+                ("s", C.c_double), ("Ps", C.c_double), ("Q", C.c_double),
+                ("Pv", C.c_double * 3), ("W", C.c_double), ("L", C.c_double * 3),
+                ("T", C.c_double), ("P", C.c_double), ("H0", C.c_double),
+                ("pot", C.c_double), ("lj", C.c_double), ("clmb", C.c_double),
+                ("wall", C.c_double), ("vir", C.c_double * 3)]
+
+
+_LIB = None
+
+
+def build_library():
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], check=True)
+
+
+def lib():
+    """Load libremd_b200.so (building it first if it is absent)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build_library()
+        L = C.CDLL(LIB_PATH)
+        L.remd_last_error.restype = C.c_char_p
+        L.remd_version.restype = C.c_char_p
+        L.remd_last_pair_count.restype = C.c_longlong
+        L.remd_create.argtypes = [C.POINTER(SystemDesc), C.c_int, _ip, C.POINTER(ReplicaInit),
+                                  C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        for fn in ["remd_destroy", "remd_compute_forces", "remd_synchronize",
+                   "remd_execute_steps_device", "remd_num_replicas",
+                   "remd_launches_per_interval", "remd_last_pair_count"]:
+            getattr(L, fn).argtypes = [C.c_void_p]
+        L.remd_execute_steps.argtypes = [C.c_void_p, _dp, _dp]
+        L.remd_execute_steps_async.argtypes = [C.c_void_p, _dp, _dp]
+        L.remd_get_averages.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.remd_get_all_averages.argtypes = [C.c_void_p, _dp]
+        L.remd_get_state.argtypes = [C.c_void_p, C.c_int, C.POINTER(StateView)]
+        L.remd_replica_nmol.argtypes = [C.c_void_p, C.c_int]
+        L.remd_replica_status.argtypes = [C.c_void_p, C.c_int, _ip]
+        L.remd_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.remd_exchange_device.argtypes = [C.c_void_p, _ip, C.c_long, _dp, C.c_ulonglong]
+        L.remd_get_conditions.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        L.remd_write_chk.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+        L.remd_wall_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, _dp]
+        L.remd_read_chk.argtypes = [C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.remd_exchange_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_long, _ip, _dp, _dp,
+                                         _dp, _dp, _dp, _ip, _ip]
+        _LIB = L
+    return _LIB
+
+
+def _check(st):
+    if st != 0:
+        raise RemdError(st, lib().remd_last_error().decode())
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def system_desc(spec) -> SystemDesc:
+    """remd_system_desc from a SystemSpec (moltype in moltype.txt units)."""
+    d = SystemDesc()
+    mt = spec.moltype
+    d.nmol, d.nsite = spec.nmol, mt.nsite
+    for k in range(mt.nsite):
+        for x in range(3):
+            d.site_r[k][x] = mt.r[k, x]
+        d.site_mass[k], d.site_sigma[k] = mt.mass[k], mt.sigma[k]
+        d.site_eps[k], d.site_charge[k] = mt.eps[k], mt.charge[k]
+    d.tconstant, d.pconstant, d.confined = spec.tconstant, spec.pconstant, spec.confined
+    d.dt_fs, d.rcut, d.rswitch = spec.dt, spec.rcut, spec.rswitch
+    d.nfwall, d.wall_length = spec.nfwall, spec.wall_length
+    d.sgm_wall, d.eps_wall, d.rho_wall = spec.sgm_wall, spec.eps_wall, spec.rho_wall
+    d.interval = spec.interval
+    return d
+
+
+class REMDGPU:
+    """All replicas of one or more ensembles on one GPU (src/remdgpu.h:92-238)."""
+
+    def __init__(self, ensembles, precision="fp32", device=0, states=None, interval=None):
+        L = lib()
+        self.ensembles = list(ensembles)
+        descs = []
+        for e in self.ensembles:
+            d = system_desc(e.spec)
+            if interval is not None:
+                d.interval = interval
+            descs.append(d)
+        n_e = len(descs)
+        self.reps_per_ens = np.array([len(e.states) for e in self.ensembles], dtype=np.int32)
+        states = states or [s for e in self.ensembles for s in e.states]
+        self._keep = []
+        inits = (ReplicaInit * len(states))()
+        for k, st in enumerate(states):
+            arrs = [np.ascontiguousarray(getattr(st, f), dtype=np.float64)
+                    for f in ("r", "v", "q", "p", "m", "I")]
+            self._keep.append(arrs)
+            ri = inits[k]
+            ri.r, ri.v, ri.q, ri.p, ri.mass, ri.inertia = [_p(a) for a in arrs]
+            ri.s, ri.Ps, ri.Q, ri.W, ri.T, ri.P = st.s, st.Ps, st.Q, st.W, st.T, st.P
+            for x in range(3):
+                ri.Pv[x] = st.Pv[x]
+                ri.L[x] = st.L[x]
+        self.nrep = len(states)
+        self.nmol = np.array([st.nmol for st in states])
+        self.h = C.c_void_p()
+        prec = 1 if precision == "fp64" else 0
+        _check(L.remd_create((SystemDesc * n_e)(*descs), n_e, _p(self.reps_per_ens, _ip), inits,
+                             prec, device, C.byref(self.h)))
+        self._keep = None
+        self.T = np.array([st.T for st in states])
+        self.P = np.array([st.P for st in states])
+
+    def close(self):
+        if self.h:
+            lib().remd_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- REMDGPU surface
+    def ExecuteSteps(self, T, P):
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        _check(lib().remd_execute_steps(self.h, _p(T), _p(P)))
+        self.T, self.P = T.copy(), P.copy()
+
+    def GetAverages(self, rep):
+        out = np.zeros(NUM_AVG)
+        _check(lib().remd_get_averages(self.h, rep, _p(out)))
+        return out
+
+    def all_averages(self):
+        out = np.zeros((self.nrep, NUM_AVG))
+        _check(lib().remd_get_all_averages(self.h, _p(out)))
+        return out
+
+    def ConvertVariablesToHost(self, rep):
+        n = int(self.nmol[rep])
+        arrs = dict(r=np.zeros((n, 3)), v=np.zeros((n, 3)), q=np.zeros((n, 4)),
+                    p=np.zeros((n, 4)), f=np.zeros((n, 3)), n=np.zeros((n, 4)))
+        sv = StateView()
+        for k, a in arrs.items():
+            setattr(sv, k, _p(a))
+        _check(lib().remd_get_state(self.h, rep, C.byref(sv)))
+        out = dict(arrs)
+        out.update(s=sv.s, Ps=sv.Ps, Q=sv.Q, Pv=np.array(sv.Pv[:]), W=sv.W, L=np.array(sv.L[:]),
+                   T=sv.T, P=sv.P, H0=sv.H0, pot=sv.pot, lj=sv.lj, clmb=sv.clmb, wall=sv.wall,
+                   vir=np.array(sv.vir[:]))
+        return out
+
+    def state(self, rep) -> ReplicaState:
+        g = self.ConvertVariablesToHost(rep)
+        n = int(self.nmol[rep])
+        return ReplicaState(g["r"], g["v"], g["q"], g["p"], np.zeros(n), np.zeros((n, 3)),
+                            g["s"], g["Ps"], g["Q"], g["Pv"], g["W"], g["L"], g["T"], g["P"])
+
+    # ---- engine extras
+    def compute_forces(self):
+        _check(lib().remd_compute_forces(self.h))
+
+    def pair_count(self):
+        return int(lib().remd_last_pair_count(self.h))
+
+    def launches_per_interval(self):
+        return int(lib().remd_launches_per_interval(self.h))
+
+    def set_tuning(self, tile, skin):
+        _check(lib().remd_set_tuning(self.h, tile, skin))
+
+    def execute_async(self, T=None, P=None):
+        if T is None:
+            _check(lib().remd_execute_steps_async(self.h, None, None))
+        else:
+            T = np.ascontiguousarray(T, dtype=np.float64)
+            P = np.ascontiguousarray(P, dtype=np.float64)
+            _check(lib().remd_execute_steps_async(self.h, _p(T), _p(P)))
+
+    def synchronize(self):
+        _check(lib().remd_synchronize(self.h))
+
+    def replica_status(self, rep):
+        s = C.c_int()
+        _check(lib().remd_replica_status(self.h, rep, C.byref(s)))
+        return s.value
+
+    def exchange_device(self, grids, step, u=None, seed=0):
+        g = np.ascontiguousarray(grids, dtype=np.int32).reshape(-1)
+        up = _p(np.ascontiguousarray(u, dtype=np.float64)) if u is not None else None
+        _check(lib().remd_exchange_device(self.h, _p(g, _ip), step, up, seed))
+
+    def execute_device(self):
+        _check(lib().remd_execute_steps_device(self.h))
+
+    def conditions(self):
+        idx = np.zeros(self.nrep, dtype=np.int32)
+        T, P = np.zeros(self.nrep), np.zeros(self.nrep)
+        _check(lib().remd_get_conditions(self.h, _p(idx, _ip), _p(T), _p(P)))
+        return idx, T, P
+
+    def write_chk(self, rep, path):
+        _check(lib().remd_write_chk(self.h, rep, path.encode()))
+
+
+def wall_table(confined, nfwall, wall_length, sgm, eps, rho):
+    out = np.zeros(2 * nfwall)
+    _check(lib().remd_wall_table(confined, nfwall, wall_length, sgm, eps, rho, _p(out)))
+    return out.reshape(nfwall, 2)
+
+
+def read_chk(path, nmol):
+    r, v, I = np.zeros((nmol, 3)), np.zeros((nmol, 3)), np.zeros((nmol, 3))
+    q, p, m, sc = np.zeros((nmol, 4)), np.zeros((nmol, 4)), np.zeros(nmol), np.zeros(10)
+    _check(lib().remd_read_chk(path.encode(), nmol, _p(r), _p(v), _p(q), _p(p), _p(m), _p(I),
+                               _p(sc)))
+    return ReplicaState(r, v, q, p, m, I, sc[0], sc[1], sc[2], sc[3:6].copy(), sc[6],
+                        sc[7:10].copy())
+
+
+def exchange_host(ntemp, npress, pconstant, step, index, T, P, pot, vol, u):
+    """REMD::ReplicaExchange on the host (in place); returns accept flags."""
+    acc = np.zeros(max(ntemp * npress // 2, 1), dtype=np.int32)
+    npairs = C.c_int()
+    _check(lib().remd_exchange_host(ntemp, npress, pconstant, step, _p(index, _ip), _p(T), _p(P),
+                                    _p(np.ascontiguousarray(pot, dtype=float)),
+                                    _p(np.ascontiguousarray(vol, dtype=float)),
+                                    _p(np.ascontiguousarray(u, dtype=float)), _p(acc, _ip),
+                                    C.byref(npairs)))
+    return acc[:npairs.value].copy()

@@ -1,0 +1,200 @@
+"""CUDA engine vs the FP64 oracle, through the C-ABI (libremd_b200.so).
+
+Tolerances (relative L2 norms over all molecules unless stated):
+  FP64 engine: forces/torques 1e-10, energies 1e-11 -- same arithmetic as the
+               oracle, different summation order;
+  FP32 engine: forces and torques 1e-5, potential energy 1e-6 (the north-star
+               accuracy gate), virial 1e-5;
+  20-step trajectories (chaotic, errors grow ~e^(t/tau)): FP64 1e-8, FP32 see
+  the per-quantity bounds in test_twenty_steps.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from remd_b200 import engine as E
+from remd_b200 import systems as S
+from remd_b200.inputs import read_chk
+from tests.common import CASES, GOLDEN, NSTEPS, golden_conditions, golden_line, golden_spec, load_case, rel
+
+pytestmark = pytest.mark.gpu
+
+SLIT_CASES = {"tip4p_slit_npxy": ("tip4p", 3, 1, 96, 201), "tip3p_slit_nvt": ("tip3p", 0, 1, 80, 202),
+              "tip5p_slit_npxy": ("tip5p", 3, 1, 72, 203)}
+
+
+def slit_case(name, interval=NSTEPS):
+    model, pcon, tcon, nmol, seed = SLIT_CASES[name]
+    e = S.small_ensemble(model=model, confined=2, nmol=nmol, ntemp=1, npress=1, seed=seed,
+                         pconstant=pcon, tconstant=tcon, interval=interval)
+    return e.spec, e.states[0]
+
+
+def any_case(name):
+    if name in CASES:
+        spec, st, _ = load_case(name)
+        return spec, st
+    return slit_case(name)
+
+
+ALL = list(CASES) + list(SLIT_CASES)
+
+
+def single(spec, st):
+    return S.Ensemble("t", spec, 1, 1, np.array([st.T]), np.array([st.P]), [st])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("name", ALL)
+def test_force_snapshot(name, prec):
+    spec, st = any_case(name)
+    eng = E.REMDGPU([single(spec, st)], precision=prec)
+    g = eng.ConvertVariablesToHost(0)
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    po = orc.prop()
+    tf = 1e-5 if prec == "fp32" else 1e-10
+    te = 1e-6 if prec == "fp32" else 1e-11
+    assert rel(g["f"], orc.f) < tf
+    assert rel(g["n"], orc.n) < tf
+    assert g["pot"] == pytest.approx(po["pot"], rel=te)
+    assert g["lj"] == pytest.approx(po["lj"], rel=te * 10)
+    assert g["clmb"] == pytest.approx(po["clmb"], rel=te)
+    assert g["wall"] == pytest.approx(po["wall"], rel=te * 10, abs=1e-9)
+    assert rel(g["vir"], po["vir"]) < tf
+    assert g["H0"] == pytest.approx(po["H0"], rel=te * 10, abs=te * 10 * abs(po["pot"]))
+    if prec == "fp64":
+        assert eng.pair_count() == po["npairs"]
+    else:
+        assert abs(eng.pair_count() - po["npairs"]) <= 1
+    eng.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("name", ALL)
+def test_twenty_steps(name, prec):
+    spec, st = any_case(name)
+    eng = E.REMDGPU([single(spec, st)], precision=prec, interval=NSTEPS)
+    eng.ExecuteSteps(np.array([st.T]), np.array([st.P]))
+    a = eng.GetAverages(0)
+    g = eng.ConvertVariablesToHost(0)
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    orc.steps(NSTEPS)
+    b = orc.average()
+    if prec == "fp64":
+        tr, tv, te = 1e-9, 1e-7, 1e-8
+    else:
+        tr, tv, te = 2e-5, 2e-3, 2e-4
+    assert rel(g["r"], orc.r) < tr
+    assert rel(g["q"], orc.q) < tr * 10
+    assert rel(g["v"], orc.v) < tv
+    assert rel(g["p"], orc.p) < tv
+    pot_a, pot_b = a[0] + a[1] + a[2], b[0] + b[1] + b[2]
+    assert pot_a == pytest.approx(pot_b, rel=te)
+    for k in [3, 4, 5, 6, 13]:   # VOL TRA ROT T TSTs
+        assert a[k] == pytest.approx(b[k], rel=te * 10), E.AVG_NAMES[k]
+    # DRF: the Hamiltonian drift, compared in absolute terms against |H0|
+    assert abs(a[12] - b[12]) < te * 10 * abs(orc.prop()["H0"]) + 1e-6
+    assert eng.replica_status(0) == 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_condition_change_applies_exchange_tail(prec):
+    """ExecuteSteps with a new (T,P) runs ChangeTemperature, KillMomentum,
+    SetPressure, CalcProperties, UpdateHamiltonian first (src/remd.cxx:526-536)."""
+    for name in ["tip4p_tube_npz", "tip3p_bulk_npt", "tip5p_slit_npxy"]:
+        spec, st = any_case(name)
+        eng = E.REMDGPU([single(spec, st)], precision=prec, interval=5)
+        T1, P1 = st.T * 1.07, st.P * 0.5 + 1e-4
+        eng.ExecuteSteps(np.array([T1]), np.array([P1]))
+        a = eng.GetAverages(0)
+        orc = O.Oracle(spec, st)
+        orc.initialize_property()
+        orc.apply_condition(T1, P1)
+        orc.steps(5)
+        b = orc.average()
+        tol = 1e-8 if prec == "fp64" else 1e-4
+        for k in [4, 5, 6, 11, 13, 14]:
+            assert a[k] == pytest.approx(b[k], rel=tol, abs=tol), (name, E.AVG_NAMES[k])
+        g = eng.ConvertVariablesToHost(0)
+        assert g["T"] == T1 and g["P"] == P1
+
+
+def test_batch_equals_alone_bitwise():
+    """Mixed ensembles in one launch: each replica's trajectory is bit-identical
+    to the same replica run alone (deterministic fixed-order reductions)."""
+    ens = [S.small_ensemble("tip3p", 0, nmol=70, ntemp=2, npress=1, seed=31, interval=10),
+           S.small_ensemble("tip4p", 1, nmol=130, ntemp=1, npress=2, seed=32, interval=10),
+           S.small_ensemble("tip5p", 2, nmol=200, ntemp=2, npress=1, seed=33, interval=10)]
+    big = E.REMDGPU(ens, precision="fp32")
+    T = np.concatenate([e.T for e in ens])
+    P = np.concatenate([e.P for e in ens])
+    big.ExecuteSteps(T, P)
+    avg = big.all_averages()
+    k = 0
+    for e in ens:
+        for j, st in enumerate(e.states):
+            one = E.REMDGPU([S.Ensemble("a", e.spec, 1, 1, e.T[j:j + 1], e.P[j:j + 1], [st])],
+                            precision="fp32")
+            one.ExecuteSteps(e.T[j:j + 1], e.P[j:j + 1])
+            assert np.array_equal(one.GetAverages(0), avg[k])
+            assert np.array_equal(one.ConvertVariablesToHost(0)["r"], big.ConvertVariablesToHost(k)["r"])
+            one.close()
+            k += 1
+
+
+def test_device_exchange_equals_host_exchange():
+    ens = [S.small_ensemble("tip4p", 0, nmol=64, ntemp=4, npress=2, seed=41, interval=5),
+           S.small_ensemble("tip3p", 1, nmol=80, ntemp=2, npress=3, seed=42, interval=5)]
+    eng = E.REMDGPU(ens, precision="fp32")
+    T = np.concatenate([e.T for e in ens])
+    P = np.concatenate([e.P for e in ens])
+    grids = [(e.ntemp, e.npress) for e in ens]
+    eng.ExecuteSteps(T, P)
+    rng = np.random.default_rng(7)
+    idx_h = [np.arange(e.nreplica, dtype=np.int32) for e in ens]
+    T_h = [e.T.copy() for e in ens]
+    P_h = [e.P.copy() for e in ens]
+    for step in range(8):
+        avg = eng.all_averages()
+        us, off = [], 0
+        for i, e in enumerate(ens):
+            pot = avg[off:off + e.nreplica, 0] + avg[off:off + e.nreplica, 1] + avg[off:off + e.nreplica, 2]
+            vol = avg[off:off + e.nreplica, 3]
+            u = rng.random(max(e.nreplica // 2, 1))
+            n = E.exchange_host(e.ntemp, e.npress, e.spec.pconstant, step, idx_h[i], T_h[i], P_h[i],
+                                pot, vol, u)
+            us.append(u[:len(n)])
+            off += e.nreplica
+        eng.exchange_device(grids, step, u=np.concatenate(us))
+        idx_d, T_d, P_d = eng.conditions()
+        assert np.array_equal(idx_d, np.concatenate(idx_h))
+        assert np.array_equal(T_d, np.concatenate(T_h)) and np.array_equal(P_d, np.concatenate(P_h))
+        eng.execute_device()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_reference_regression_input(prec):
+    """test/input/gpu0000.chk through the engine: interval 0 against the
+    reference's golden line (loose band) and the oracle (tight)."""
+    spec = golden_spec()
+    st = read_chk(f"{GOLDEN}/gpu0000.chk")
+    st.T, st.P = golden_conditions()
+    orc = O.Oracle(spec, st)
+    orc.velocity_scaling()
+    orc.ang_velocity_scaling()
+    orc.set_tstat_mass(0.5)
+    st0 = orc.state()
+    orc.initialize_property()
+    orc.steps(100)
+    b = orc.average()
+    eng = E.REMDGPU([single(spec, st0)], precision=prec)
+    eng.ExecuteSteps(np.array([st0.T]), np.array([st0.P]))
+    a = eng.GetAverages(0)
+    g = dict(zip(golden_line()["columns"], golden_line()["values"]))
+    assert a[0] + a[1] + a[2] == pytest.approx(g["pot"], rel=2e-4)
+    assert a[3] == pytest.approx(g["vol"], rel=2e-4)
+    tol = 1e-8 if prec == "fp64" else 1e-4
+    assert a[0] + a[1] + a[2] == pytest.approx(b[0] + b[1] + b[2], rel=tol)
+    assert a[3] == pytest.approx(b[3], rel=tol)

@@ -1,0 +1,98 @@
+"""The C oracle restates the reference's generic FP64 CPU path.  These tests pin
+it against (a) fixtures the reference itself produced (tests/golden/ref_*.npz,
+made by tests/golden/make_golden.py) and (b) the compiled reference, when
+oracle/_ref is present."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.common import CASES, NSTEPS, load_case, rel
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_force_snapshot_matches_reference(name):
+    spec, st, z = load_case(name)
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    assert rel(orc.f, z["snap_f"]) < 1e-13
+    assert rel(orc.n, z["snap_n"]) < 1e-12
+    p = orc.prop()
+    e = z["snap_ener"]
+    assert p["lj"] == pytest.approx(e[0], rel=1e-13)
+    assert p["clmb"] == pytest.approx(e[1], rel=1e-13)
+    assert p["wall"] == pytest.approx(e[2], rel=1e-13, abs=1e-12)
+    assert np.allclose(p["vir"], e[3:6], rtol=1e-12, atol=1e-9)
+    assert p["tra"] == pytest.approx(e[6], rel=1e-13)
+    assert p["rot"] == pytest.approx(e[7], rel=1e-13)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_twenty_steps_match_reference(name):
+    spec, st, z = load_case(name)
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    orc.steps(NSTEPS)
+    # identical arithmetic up to the reference's uninitialised bulk wall term
+    assert rel(orc.r, z["after_r"]) < 1e-12
+    assert rel(orc.v, z["after_v"]) < 1e-10
+    assert rel(orc.q, z["after_q"]) < 1e-12
+    assert rel(orc.p, z["after_p"]) < 1e-10
+    assert rel(orc.f, z["after_f"]) < 1e-9
+    p = orc.prop()
+    sc = z["after_scal"]
+    assert p["s"] == pytest.approx(sc[0], rel=1e-11)
+    assert p["Ps"] == pytest.approx(sc[1], rel=1e-8, abs=1e-10)
+    assert np.allclose(p["Pv"], sc[2:5], rtol=1e-8, atol=1e-10)
+    assert np.allclose(p["L"], sc[5:8], rtol=1e-13)
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref not built (no reference sources)")
+@pytest.mark.parametrize("name", ["tip4p_tube_npz", "tip3p_bulk_npt"])
+def test_live_reference_bitwise(name):
+    """With the same compiler flags the restatement is bit-identical for tube systems."""
+    spec, st, _ = load_case(name)
+    ref = O.Reference(spec, st, spec.moltype_file)
+    orc = O.Oracle(spec, st)
+    ref.initialize_property()
+    orc.initialize_property()
+    ref.execute_steps(5)
+    orc.steps(5)
+    g = ref.get()
+    pr, po = ref.prop(), orc.prop()
+    if spec.confined:
+        assert np.array_equal(g["r"], orc.r) and np.array_equal(g["p"], orc.p)
+        assert np.array_equal(g["f"], orc.f) and np.array_equal(g["n"], orc.n)
+        assert (pr["lj"], pr["clmb"], pr["wall"]) == (po["lj"], po["clmb"], po["wall"])
+    else:
+        assert rel(g["r"], orc.r) < 1e-13
+        assert pr["lj"] == pytest.approx(po["lj"], rel=1e-12)
+
+
+def test_exchange_matches_reference_remdinfo():
+    """REMD::ReplicaExchange restatement vs the reference's REMDInfo pair lists."""
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(5)
+    nt, npr = 4, 2
+    inp = ("nmol 64\nntemp %d\nnpress %d\nnreplica %d\ntemp_min 250\ntemp_max 350\n"
+           "press_min 1e5\npress_max 2e8\npconstant 1\nconfined 0\ntconstant 1\n" % (nt, npr, nt * npr))
+    lib = O._ref_lib()
+    h = lib.ref_remdinfo_create(inp.encode())
+    n = nt * npr
+    idx_r = np.zeros(n, dtype=np.int32)
+    T_r, P_r = np.zeros(n), np.zeros(n)
+    lib.ref_remdinfo_arrays(h, O._ptr(idx_r, O._ip), O._ptr(T_r), O._ptr(P_r))
+    T_o, P_o = O.conditions_geometrical(nt, npr, 250, 350, 1e5, 2e8)
+    assert np.array_equal(T_o, T_r) and np.array_equal(P_o, P_r)
+    idx_o = np.arange(n, dtype=np.int32)
+    for step in range(24):
+        pot = rng.normal(-4000, 30, n)
+        vol = rng.normal(3000, 20, n)
+        u = rng.random(n)
+        acc_r = np.zeros(n, dtype=np.int32)
+        lib.ref_remdinfo_exchange(h, step, O._ptr(pot), O._ptr(vol), O._ptr(u), O._ptr(acc_r, O._ip))
+        acc_o = O.replica_exchange(nt, npr, 1, step, idx_o, T_o, P_o, pot, vol, u)
+        lib.ref_remdinfo_arrays(h, O._ptr(idx_r, O._ip), O._ptr(T_r), O._ptr(P_r))
+        assert np.array_equal(acc_o, acc_r[:len(acc_o)])
+        assert np.array_equal(idx_o, idx_r)
+        assert np.array_equal(T_o, T_r) and np.array_equal(P_o, P_r)
