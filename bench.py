@@ -61,6 +61,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
+    ap.add_argument("--equil-rounds", type=int, default=10,
+                    help="untimed relaxation rounds of 20 steps + init_scaling")
     return ap.parse_args(argv)
 
 
@@ -276,6 +278,8 @@ def engine_arm(args, rank, world, local):
     mol_steps_per_interval = nmol_total * args.interval
     stream = torch.cuda.ExternalStream(E.lib().remd_stream(eng.h))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+    # untimed: relax the lattice start (init_scaling every 20 steps), then warm up
+    eng.equilibrate(rounds=args.equil_rounds, steps=20)
     for _ in range(args.warmup):
         eng.execute_async(T, P)
     eng.synchronize()

@@ -135,6 +135,18 @@ remd_status remd_execute_steps(remd_handle h, const double *T, const double *P);
 remd_status remd_execute_steps_async(remd_handle h, const double *T, const double *P);
 remd_status remd_synchronize(remd_handle h);
 
+/* Advance every replica by nsteps MD steps (kernels launched one by one; the
+ * interval start/end bookkeeping as in remd_execute_steps, conditions as left
+ * by the last call).  Molecules::ExecuteSteps with interval = nsteps
+ * (src/integrator.cxx:708-803). */
+remd_status remd_execute_nsteps(remd_handle h, int nsteps);
+
+/* The reference's init_scaling for every replica: Molecules::VelocityScaling
+ * and AngVelocityScaling (src/molecules.cxx:262-307) -- kinetic energies set to
+ * 1.5 N T, momentum removed, s=1, Ps=0, Pv=0 -- then H0 recomputed as in
+ * InitializeProperty (src/molecules.h:260-270). */
+remd_status remd_rescale_velocities(remd_handle h);
+
 /* Replaces REMDGPU::GetAverages(rep) (src/remdgpu.h:208-233): the 19 fields of
  * Average for replica `rep` after the last ExecuteSteps (T and P reduced). */
 remd_status remd_get_averages(remd_handle h, int rep, double out[REMD_NUM_AVERAGES]);

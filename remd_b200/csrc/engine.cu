@@ -562,6 +562,25 @@ remd_status remd_execute_steps_device(remd_handle h) {
   return sync_and_check(h);
 }
 
+remd_status remd_execute_nsteps(remd_handle h, int nsteps) {
+  if (!h || nsteps < 1) { set_error("remd_execute_nsteps: nsteps must be >= 1"); return REMD_ERR_INVALID; }
+  launch_replica_start(h->d, h->X, h->stream);
+  for (int s = 0; s < nsteps; s++) {
+    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
+  }
+  launch_replica_end(h->d, h->X, h->stream);
+  CK(cudaGetLastError());
+  return sync_and_check(h);
+}
+
+remd_status remd_rescale_velocities(remd_handle h) {
+  if (!h) return REMD_ERR_INVALID;
+  launch_replica_rescale(h->d, h->X, h->stream);
+  CK(cudaGetLastError());
+  return sync_and_check(h);
+}
+
 remd_status remd_get_averages(remd_handle h, int rep, double* out) {
   if (!h || !out || rep < 0 || rep >= h->nrep) { set_error("remd_get_averages: bad argument"); return REMD_ERR_INVALID; }
   CK(cudaStreamSynchronize(h->stream));

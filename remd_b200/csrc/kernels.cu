@@ -790,6 +790,59 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_props(DevPtrs d, RepSta
   }
 }
 
+// Molecules::KillMomentum + KillAngularMomentumInTube (src/molecules.cxx:168-210)
+// for the replica of this block; L and s from st.
+__device__ void kill_momentum_block(const DevPtrs& d, const RepConst& c, const RepState& st,
+                                    double* red, bool tube_angular) {
+  const int N = d.N;
+  double acc[4] = {0, 0, 0, 0};
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    for (int x = 0; x < 3; x++) acc[x] += d.v[x * N + g] * c.mass;
+    acc[3] += c.mass;
+  }
+  block_sum<4>(acc, red);
+  const double mom[3] = {acc[0] / acc[3], acc[1] / acc[3], acc[2] / acc[3]};
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    if (c.confined == 1) {
+      d.v[2 * N + g] -= mom[2];
+    } else if (c.confined == 2) {
+      d.v[g] -= mom[0];
+      d.v[N + g] -= mom[1];
+    } else {
+      for (int x = 0; x < 3; x++) d.v[x * N + g] -= mom[x];
+    }
+  }
+  __syncthreads();
+  if (c.confined == 1 && tube_angular) {
+    double am[4] = {0, 0, 0, 0};
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+      const int g = c.mol_off + li;
+      double r[3], v[3];
+      for (int x = 0; x < 3; x++) {
+        r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+        v[x] = d.v[x * N + g] / (st.L[x] * st.s);
+      }
+      am[0] += c.mass * (r[0] * v[1] - r[1] * v[0]);
+      am[1] += c.mass;
+    }
+    block_sum<4>(am, red);
+    const double lz = am[0] / am[1];
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+      const int g = c.mol_off + li;
+      double r[3];
+      for (int x = 0; x < 3; x++) r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+      const double r02 = r[0] * r[0] + r[1] * r[1];
+      if (r02 > 1.0) {
+        d.v[g] += lz * r[1] / r02 * st.L[0] * st.s;
+        d.v[N + g] -= lz * r[0] / r02 * st.L[1] * st.s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The exchange tail for a replica whose condition changed (src/remd.cxx:526-536):
 // ChangeTemperature (src/molecules.h:333-353), KillMomentum (+ the tube's angular
 // momentum, src/molecules.cxx:168-210), SetPressure, CalcProperties, UpdateHamiltonian.
@@ -820,57 +873,13 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
   __syncthreads();
   const int N = d.N;
   const double sc = sh[0];
-  double acc[4] = {0, 0, 0, 0};
   for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
     const int g = c.mol_off + li;
-    for (int x = 0; x < 3; x++) {
-      const double v = d.v[x * N + g] * sc;
-      d.v[x * N + g] = v;
-      acc[x] += v * c.mass;
-    }
+    for (int x = 0; x < 3; x++) d.v[x * N + g] *= sc;
     for (int x = 0; x < 4; x++) d.p[x * N + g] *= sc;
-    acc[3] += c.mass;
-  }
-  block_sum<4>(acc, red);
-  const double mom[3] = {acc[0] / acc[3], acc[1] / acc[3], acc[2] / acc[3]};
-  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
-    const int g = c.mol_off + li;
-    if (c.confined == 1) {
-      d.v[2 * N + g] -= mom[2];
-    } else if (c.confined == 2) {
-      d.v[g] -= mom[0];
-      d.v[N + g] -= mom[1];
-    } else {
-      for (int x = 0; x < 3; x++) d.v[x * N + g] -= mom[x];
-    }
   }
   __syncthreads();
-  if (c.confined == 1) {   // KillAngularMomentumInTube
-    double am[4] = {0, 0, 0, 0};
-    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
-      const int g = c.mol_off + li;
-      double r[3], v[3];
-      for (int x = 0; x < 3; x++) {
-        r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
-        v[x] = d.v[x * N + g] / (st.L[x] * st.s);
-      }
-      am[0] += c.mass * (r[0] * v[1] - r[1] * v[0]);
-      am[1] += c.mass;
-    }
-    block_sum<4>(am, red);
-    const double lz = am[0] / am[1];
-    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
-      const int g = c.mol_off + li;
-      double r[3];
-      for (int x = 0; x < 3; x++) r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
-      const double r02 = r[0] * r[0] + r[1] * r[1];
-      if (r02 > 1.0) {
-        d.v[g] += lz * r[1] / r02 * st.L[0] * st.s;
-        d.v[N + g] -= lz * r[0] / r02 * st.L[1] * st.s;
-      }
-    }
-    __syncthreads();
-  }
+  kill_momentum_block(d, c, st, red, true);
   double kacc[4];
   kinetic_sums(d, c, st.s, kacc);
   block_sum<4>(kacc, red);
@@ -878,6 +887,61 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
     RepState s = st;
     s.P = Pn;
     s.H0 = calc_properties(d, c, s, kacc, kacc[3], nullptr);
+    X[rep] = s;
+  }
+}
+
+// Molecules::VelocityScaling + AngVelocityScaling (src/molecules.cxx:262-307), the
+// reference's init_scaling: translational and rotational kinetic energies set to
+// 1.5 N T each, momentum removed, thermostat and barostat momenta reset, then H0
+// recomputed (InitializeProperty).
+__global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepState* X) {
+  __shared__ RepState st;
+  __shared__ double red[8 * 4];
+  const int rep = blockIdx.x;
+  const RepConst& c = d.rc[rep];
+  if (threadIdx.x == 0) st = X[rep];
+  __syncthreads();
+  const int N = d.N;
+  double k[4];
+  kinetic_sums(d, c, st.s, k);
+  block_sum<4>(k, red);
+  {
+    double tra = 0.0;
+    for (int x = 0; x < 3; x++) {
+      const double cf = 1.0 / (st.L[x] * st.s);
+      tra += k[x] * (cf * cf * 0.5);
+    }
+    const double coef = (tra > 0.0) ? sqrt(1.5 * c.nmol * st.T / tra) : 1.0;
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x)
+      for (int x = 0; x < 3; x++) d.v[x * N + c.mol_off + li] *= coef;
+  }
+  __syncthreads();
+  kill_momentum_block(d, c, st, red, true);
+  if (c.confined == 1) kill_momentum_block(d, c, st, red, true);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st.s = 1.0;
+    st.Ps = 0.0;
+    st.Pv[0] = st.Pv[1] = st.Pv[2] = 0.0;
+  }
+  __syncthreads();
+  kinetic_sums(d, c, st.s, k);
+  block_sum<4>(k, red);
+  {
+    const double coef = (k[3] > 0.0) ? sqrt(1.5 * c.nmol * st.T / k[3]) : 1.0;
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x)
+      for (int x = 0; x < 4; x++) d.p[x * N + c.mol_off + li] *= coef;
+  }
+  __syncthreads();
+  kinetic_sums(d, c, st.s, k);
+  block_sum<4>(k, red);
+  if (threadIdx.x == 0) {
+    RepState s = st;
+    s.gkT = 6.0 * (double)c.nmol * s.T;
+    double* avg = d.avg + (long long)rep * kNumAvg;
+    s.H0 = calc_properties(d, c, s, k, k[3], avg);
+    avg[12] = 0.0;
     X[rep] = s;
   }
 }
@@ -1028,6 +1092,9 @@ void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s) {
 }
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s) {
   k_replica_props<<<d.nrep, kRepThreads, 0, s>>>(d, X);
+}
+void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s) {
+  k_replica_rescale<<<d.nrep, kRepThreads, 0, s>>>(d, X);
 }
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, unsigned long long seed, int* index,

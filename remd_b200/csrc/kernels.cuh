@@ -30,6 +30,7 @@ void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int pre
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);
+void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, unsigned long long seed, int* index,
                        double* T, double* P, cudaStream_t s);

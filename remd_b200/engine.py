@@ -88,6 +88,14 @@ def lib():
                    "remd_launches_per_interval", "remd_last_pair_count"]:
             getattr(L, fn).argtypes = [C.c_void_p]
         L.remd_execute_steps.argtypes = [C.c_void_p, _dp, _dp]
+        L.remd_execute_nsteps.argtypes = [C.c_void_p, C.c_int]
+        L.remd_rescale_velocities.argtypes = [C.c_void_p]
+        L.remd_replica_pair_count.restype = C.c_longlong
+        L.remd_replica_pair_count.argtypes = [C.c_void_p, C.c_int]
+        L.remd_stream.restype = C.c_void_p
+        L.remd_stream.argtypes = [C.c_void_p]
+        L.remd_profile_steps.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.remd_measure_fp32_peak.argtypes = [C.c_int, _dp]
         L.remd_execute_steps_async.argtypes = [C.c_void_p, _dp, _dp]
         L.remd_get_averages.argtypes = [C.c_void_p, C.c_int, _dp]
         L.remd_get_all_averages.argtypes = [C.c_void_p, _dp]
@@ -220,6 +228,22 @@ class REMDGPU:
                             g["s"], g["Ps"], g["Q"], g["Pv"], g["W"], g["L"], g["T"], g["P"])
 
     # ---- engine extras
+    def execute_nsteps(self, n):
+        _check(lib().remd_execute_nsteps(self.h, n))
+
+    def rescale_velocities(self):
+        """The reference's init_scaling (VelocityScaling + AngVelocityScaling)."""
+        _check(lib().remd_rescale_velocities(self.h))
+
+    def equilibrate(self, rounds=10, steps=20):
+        """Relax a lattice start: `rounds` x (`steps` MD steps, then init_scaling)."""
+        for _ in range(rounds):
+            self.execute_nsteps(steps)
+            self.rescale_velocities()
+
+    def replica_pair_count(self, rep):
+        return int(lib().remd_replica_pair_count(self.h, rep))
+
     def compute_forces(self):
         _check(lib().remd_compute_forces(self.h))
 
