@@ -144,7 +144,8 @@ remd_status remd_execute_nsteps(remd_handle h, int nsteps);
 /* The reference's init_scaling for every replica: Molecules::VelocityScaling
  * and AngVelocityScaling (src/molecules.cxx:262-307) -- kinetic energies set to
  * 1.5 N T, momentum removed, s=1, Ps=0, Pv=0 -- then H0 recomputed as in
- * InitializeProperty (src/molecules.h:260-270). */
+ * InitializeProperty (src/molecules.h:260-270).  v and p are first divided by
+ * s (a no-op at start-up, where the reference calls it with s = 1). */
 remd_status remd_rescale_velocities(remd_handle h);
 
 /* Replaces REMDGPU::GetAverages(rep) (src/remdgpu.h:208-233): the 19 fields of

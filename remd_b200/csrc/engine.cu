@@ -387,6 +387,10 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
       }
       for (int k = 0; k < s.nsite; k++)
         for (int l = 0; l < s.nsite; l++) c.qq[k][l] = qr[k] * qr[l];
+      c.site_reach = 0.0;
+      for (int k = 0; k < s.nsite; k++)
+        c.site_reach = std::max(c.site_reach, std::sqrt(c.body[k][0] * c.body[k][0] + c.body[k][1] * c.body[k][1] +
+                                                        c.body[k][2] * c.body[k][2]));
       const double sg = 0.5 * (s.site_sigma[0] * (1e-10 / unit_length()) * 2.0);
       c.sgm2 = sg * sg;
       const double eo = s.site_eps[0] * (1e+03 / 6.0221367e+23 / unit_energy());

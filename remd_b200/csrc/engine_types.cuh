@@ -49,6 +49,8 @@ struct RepConst {
   double body[kMaxSites][3];
   double qq[kMaxSites][kMaxSites];
   double sgm2, eps;        // O-O Lennard-Jones: ((s+s)/2)^2 and sqrt(e e)
+  double site_reach;       // max |site - centre of mass| (A): per-site images matter
+                           // once L_d < 2 (rc + 2 site_reach)
 };
 
 // Per-replica scalars (two copies, ping-pong).

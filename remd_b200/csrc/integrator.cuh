@@ -52,8 +52,11 @@ __device__ inline void d4(const RepConst& c, RepState& st) {
   if (c.pconstant == 1) {
     if (c.tconstant == 1) st.Ps -= st.Pv[0] * st.Pv[0] / c.W * dthalf;
     const double V = volume(c, st);
-    // the reference takes the cube root in single precision (powf)
-    const double Ln = (double)powf((float)(V + st.Pv[0] * st.s / c.W * dthalf), (float)(1. / 3.));
+    // the reference takes the cube root in single precision (powf(float, float),
+    // src/integrator.cxx:614); evaluated here in double and rounded once to
+    // float, i.e. the correctly rounded single-precision result
+    const float xf = (float)(V + st.Pv[0] * st.s / c.W * dthalf);
+    const double Ln = (double)(float)pow((double)xf, (double)(float)(1. / 3.));
     st.L[0] = st.L[1] = st.L[2] = Ln;
   }
   if (c.pconstant == 2) {

@@ -304,9 +304,13 @@ struct IAcc {
   long long npair;
 };
 
-// FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU),
-// partial sums in FP32 over at most 16 neighbours, then FP64 accumulation.
-template <int S, int C0>
+// FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU
+// plus one Newton step), partial sums in FP32 over at most 4 neighbours, then
+// FP64 accumulation.
+// SIMG: apply the minimum image to every site pair as the reference does
+// (src/force_calculator.cxx:737-741).  It changes the result only when a box
+// length is below 2 (rc + 2 site_reach); the caller enables it just then.
+template <int S, int C0, bool SIMG>
 __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                               const uint16_t* nb, int cnt, IAcc& a) {
   constexpr int STRIDE = ((3 + 3 * S) + 3) / 4 * 4;
@@ -334,6 +338,8 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
     for (int l = 0; l < S; l++) qq[k][l] = (float)c.qq[k][l];
   const float Lsx = (float)(L[0] * kFixInv), Lsy = (float)(L[1] * kFixInv),
               Lsz = (float)(L[2] * kFixInv);
+  const float Lfx = (float)L[0], Lfy = (float)L[1], Lfz = (float)L[2];
+  const float hLx = 0.5f * Lfx, hLy = 0.5f * Lfy, hLz = 0.5f * Lfz;
   const float rc = (float)c.rc, rs = (float)c.rs, rc2 = (float)(c.rc * c.rc);
   const float coef = (float)c.coef_sw;
   const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
@@ -398,9 +404,18 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
           const bool lj_pair = (kk == 0 && l == 0);
           const bool cl_pair = (kk >= C0 && l >= C0);
           if (!lj_pair && !cl_pair) continue;
-          const float x = ax - sj[l][0], y = ay - sj[l][1], z = az - sj[l][2];
+          float x = ax - sj[l][0], y = ay - sj[l][1], z = az - sj[l][2];
+          if (SIMG) {
+            if (x >= hLx) x -= Lfx;
+            if (x < -hLx) x += Lfx;
+            if (y >= hLy) y -= Lfy;
+            if (y < -hLy) y += Lfy;
+            if (z >= hLz) z -= Lfz;
+            if (z < -hLz) z += Lfz;
+          }
           const float rr = x * x + y * y + z * z;
-          const float ri = rsqrtf(rr);
+          float ri = rsqrtf(rr);
+          ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);   // one Newton step: ~0.5 ulp
           const float ri2 = ri * ri;
           float ftmp = 0.f;
           if (lj_pair) {
@@ -430,7 +445,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
       flj += sw * elj;
       fcl += sw * ecl;
     }
-    if ((k & 15) == 15) { flush(); zero(); }
+    if ((k & 3) == 3) { flush(); zero(); }
   }
   flush();
   a.npair += np;
@@ -438,7 +453,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 
 // FP64 pair loop: the reference's generic Switching (src/force_calculator.cxx:691-779)
 // arithmetic for molecule i, over its neighbour list.
-template <int S, int C0>
+template <int S, int C0, bool SIMG>
 __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                               const uint16_t* nb, int cnt, IAcc& a) {
   constexpr int STRIDE = ((3 + 3 * S) + 1) / 2 * 2;
@@ -479,7 +494,13 @@ __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t
         const bool cl_pair = (kk >= C0 && l >= C0);
         if (!lj_pair && !cl_pair) continue;
         double rv[3];
-        for (int x = 0; x < 3; x++) rv[x] = gr[x] + wi[3 + 3 * kk + x] - wj[3 + 3 * l + x];
+        for (int x = 0; x < 3; x++) {
+          rv[x] = gr[x] + wi[3 + 3 * kk + x] - wj[3 + 3 * l + x];
+          if (SIMG) {
+            if (rv[x] >= 0.5 * L[x]) rv[x] -= L[x];
+            if (rv[x] < -0.5 * L[x]) rv[x] += L[x];
+          }
+        }
         const double rr = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
         const double r02i = 1.0 / rr;
         const double r01i = sqrt(r02i);
@@ -547,10 +568,15 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
   double wall_e = 0.0;
   if (valid) {
     const int cnt = d.nbr_cnt[g];
-    if (PREC == kF32)
-      pair_loop_f32<S, C0>(d, c, t, L, nb, cnt, a);
-    else
-      pair_loop_f64<S, C0>(d, c, t, L, nb, cnt, a);
+    const double reach = c.rc + 2.0 * c.site_reach;
+    const bool simg = (L[0] < 2.0 * reach) || (L[1] < 2.0 * reach) || (L[2] < 2.0 * reach);
+    if (PREC == kF32) {
+      if (simg) pair_loop_f32<S, C0, true>(d, c, t, L, nb, cnt, a);
+      else pair_loop_f32<S, C0, false>(d, c, t, L, nb, cnt, a);
+    } else {
+      if (simg) pair_loop_f64<S, C0, true>(d, c, t, L, nb, cnt, a);
+      else pair_loop_f64<S, C0, false>(d, c, t, L, nb, cnt, a);
+    }
     const int N = d.N;
     double q[4], r[3];
     for (int x = 0; x < 4; x++) q[x] = d.q[x * N + g];
@@ -894,7 +920,10 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
 // Molecules::VelocityScaling + AngVelocityScaling (src/molecules.cxx:262-307), the
 // reference's init_scaling: translational and rotational kinetic energies set to
 // 1.5 N T each, momentum removed, thermostat and barostat momenta reset, then H0
-// recomputed (InitializeProperty).
+// recomputed (InitializeProperty).  The stored v and p carry a factor s; they
+// are first brought to s = 1 (the reference calls this only at start-up, where
+// s = 1 already, and resetting s afterwards would otherwise scale the kinetic
+// energy by 1/s^2).
 __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepState* X) {
   __shared__ RepState st;
   __shared__ double red[8 * 4];
@@ -903,6 +932,17 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepS
   if (threadIdx.x == 0) st = X[rep];
   __syncthreads();
   const int N = d.N;
+  if (st.s != 1.0) {
+    const double si = 1.0 / st.s;
+    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+      const int g = c.mol_off + li;
+      for (int x = 0; x < 3; x++) d.v[x * N + g] *= si;
+      for (int x = 0; x < 4; x++) d.p[x * N + g] *= si;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) st.s = 1.0;
+    __syncthreads();
+  }
   double k[4];
   kinetic_sums(d, c, st.s, k);
   block_sum<4>(k, red);

@@ -285,10 +285,30 @@ def config3(seed=3):
 CONFIG4_GRIDS = [(16, 4), (12, 4), (8, 4), (16, 2), (6, 4), (12, 2), (8, 2), (4, 4)]
 
 
+def feasible_periodic_length(confined, nmol, wall):
+    """Shortest periodic length of the liquid-density lattice start (A)."""
+    if confined == 0:
+        return math.ceil(nmol ** (1.0 / 3.0) - 1e-9) * 3.1
+    if confined == 1:
+        racc = max(wall - 2.6, 0.0)
+        m = int(racc // 2.9)
+        k = sum(1 for i in range(-m, m + 1) for j in range(-m, m + 1)
+                if (i * 2.9) ** 2 + (j * 2.9) ** 2 <= racc ** 2 + 1e-9)
+        return math.ceil(nmol / k) * 3.0
+    zacc = max(wall / 2.0 - 1.8, 0.0)
+    nz = int(2 * zacc // 2.9) + 1
+    return math.ceil(math.sqrt(nmol / nz)) * 3.1
+
+
 def config4(seed=4, interval=100):
     """8 ensembles, 256 replicas: nmol log-uniform 64-2048, models uniform over
     TIP3P/4P/5P, confinement uniform over bulk/tube (R 4-8 A)/slit (7-14 A),
-    rc 8.5-12 (rs = rc-1 or rc-2), grids over 200-400 K x 0.1-300 MPa."""
+    rc 8.5-12 (rs = rc-1 or rc-2), grids over 200-400 K x 0.1-300 MPa.
+
+    A drawn (confinement, rc) whose liquid-density lattice would have a
+    periodic length below 2*rc+2 A (the minimum-image bound) gets the largest
+    feasible rc >= 8.5 A; if none exists the system becomes a nanotube, whose
+    periodic length grows with nmol.  So no system is inflated to gas density."""
     rng = np.random.default_rng(seed)
     grids = [CONFIG4_GRIDS[i] for i in rng.permutation(len(CONFIG4_GRIDS))]
     out = []
@@ -296,12 +316,20 @@ def config4(seed=4, interval=100):
         nmol = int(round(math.exp(rng.uniform(math.log(64), math.log(2048)))))
         model = ["tip3p", "tip4p", "tip5p"][rng.integers(3)]
         confined = int(rng.integers(3))
-        wall = float(rng.uniform(4.0, 8.0)) if confined == 1 else \
-            float(rng.uniform(7.0, 14.0)) if confined == 2 else 0.0
+        tube_r = float(rng.uniform(4.0, 8.0))
+        slit_w = float(rng.uniform(7.0, 14.0))
         rc = float(rng.uniform(8.5, 12.0))
-        rs = rc - float(rng.choice([1.0, 2.0]))
-        out.append(make_ensemble(f"config4.{e}", model, confined, nmol, wall, rc, rs, nt, npr,
-                                 200, 400, 0.1e6, 300e6, seed * 1000 + e, interval=interval))
+        drs = float(rng.choice([1.0, 2.0]))
+        wall = tube_r if confined == 1 else slit_w if confined == 2 else 0.0
+        Lp = feasible_periodic_length(confined, nmol, wall)
+        if Lp < 2.0 * rc + 2.0:
+            rc = (Lp - 2.0) / 2.0
+            if rc < 8.5:
+                confined, wall, rc = 1, tube_r, float(rng.uniform(8.5, 12.0))
+                while feasible_periodic_length(1, nmol, wall) < 2.0 * rc + 2.0:
+                    wall -= 0.25
+        out.append(make_ensemble(f"config4.{e}", model, confined, nmol, wall, rc, rc - drs, nt,
+                                 npr, 200, 400, 0.1e6, 300e6, seed * 1000 + e, interval=interval))
     return out
 
 
