@@ -5,7 +5,8 @@ Workload (default): the 256-replica uneven batch -- 8 seeded ensembles, nmol
 log-uniform in 64..2048, TIP3P/TIP4P/TIP5P, bulk / nanotube / nano-slit, rcut
 8.5..12 A (remd_b200.systems.config4) -- with interval = 100 MD steps.  One
 bench "step" is one REMD interval of the whole batch: 100 MD steps of every
-replica (integrator, forces, wall) plus the interval start/end kernels.
+replica (integrator, forces, wall), the interval start/end kernels and the
+Metropolis T/P exchange of every ensemble, captured as one CUDA graph.
 
   value      whole-job mol-steps/s with the state resident in HBM, timed with
              CUDA events on the engine's stream (sum over the K intervals), L2
@@ -280,6 +281,9 @@ def engine_arm(args, rank, world, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
     # untimed: relax the lattice start (init_scaling every 20 steps), then warm up
     eng.equilibrate(rounds=args.equil_rounds, steps=20)
+    # one bench step = one REMD interval: `interval` MD steps of every replica and
+    # the Metropolis exchange of every ensemble, all on the device
+    eng.enable_device_exchange([(e.ntemp, e.npress) for e in ens], seed=2024 + rank)
     for _ in range(args.warmup):
         eng.execute_async(T, P)
     eng.synchronize()
@@ -335,6 +339,7 @@ def engine_arm(args, rank, world, local):
 
     # end to end through the public C-ABI call (host buffers, host exchange)
     e2e = None
+    eng.enable_device_exchange(None)
     if not args.no_e2e:
         grids = [(e.ntemp, e.npress) for e in ens]
         idx = [np.arange(e.nreplica, dtype=np.int32) for e in ens]

@@ -217,6 +217,14 @@ remd_status remd_exchange_device(remd_handle h, const int *grids, long step, con
 /* Advance one interval with the conditions left on the device by
  * remd_exchange_device (no host round trip). */
 remd_status remd_execute_steps_device(remd_handle h);
+/* Append the Metropolis exchange of every ensemble to each interval run by
+ * remd_execute_steps_async/_device (one REMD interval = interval MD steps +
+ * the exchange, REMD::ExecuteREMD, src/remd.cxx:297-441), with a per-ensemble
+ * step counter starting at first_step and Philox uniforms from seed.  grids =
+ * NULL turns it off.  Conditions chosen by the exchange are applied at the
+ * start of the next interval. */
+remd_status remd_enable_device_exchange(remd_handle h, const int *grids, unsigned long long seed,
+                                        long long first_step);
 /* Read back the device-side condition arrays (index per ensemble slot, T, P per replica). */
 remd_status remd_get_conditions(remd_handle h, int *index, double *T, double *P);
 

@@ -50,6 +50,10 @@ struct remd_engine_s {
   int u_cap = 0;
   cudaGraphExec_t gexec = nullptr;
   int graph_tile = 0;
+  bool graph_exchange = false;
+  bool exch_enabled = false;        // device exchange appended to every interval
+  unsigned long long exch_seed = 0;
+  long long* d_step = nullptr;      // per-ensemble interval counter of the device exchange
   long long last_pairs = 0;
   size_t bytes = 0;
 };
@@ -137,6 +141,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       nr * 4,                          // 23 index
       (size_t)h->nens * 2 * 4, (size_t)h->nens * 4, (size_t)h->nens * 4,   // 24 grid 25 rep_off 26 u_off
       (size_t)std::max(nr / 2, (size_t)1) * 8,   // 27 u
+      (size_t)h->nens * 8,             // 28 per-ensemble exchange step counter
   };
   offs.clear();
   total = 0;
@@ -194,6 +199,7 @@ static remd_status allocate(remd_engine_s* h) {
   h->d_rep_off = reinterpret_cast<int*>(b + offs[25]);
   h->d_u_off = reinterpret_cast<int*>(b + offs[26]);
   h->d_u = reinterpret_cast<double*>(b + offs[27]);
+  h->d_step = reinterpret_cast<long long*>(b + offs[28]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
@@ -252,6 +258,9 @@ static remd_status build_graph(remd_engine_s* h) {
     launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
   }
   launch_replica_end(h->d, h->X, h->stream);
+  if (h->exch_enabled)
+    launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, -1, nullptr, h->exch_seed,
+                      h->d_index, h->dT, h->dP, h->d_step, h->stream);
   cudaError_t le = cudaGetLastError();
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
   if (le != cudaSuccess || ce != cudaSuccess) {
@@ -265,6 +274,7 @@ static remd_status build_graph(remd_engine_s* h) {
     return REMD_ERR_CUDA;
   }
   h->graph_tile = h->tile;
+  h->graph_exchange = h->exch_enabled;
   return REMD_OK;
 }
 
@@ -536,7 +546,7 @@ remd_status remd_execute_steps_async(remd_handle h, const double* T, const doubl
     CK(cudaMemcpyAsync(h->dT, h->hT, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->dP, h->hP, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
   }
-  if (!h->gexec || h->graph_tile != h->tile) {
+  if (!h->gexec || h->graph_tile != h->tile || h->graph_exchange != h->exch_enabled) {
     remd_status s = build_graph(h);
     if (s != REMD_OK) return s;
   }
@@ -733,9 +743,30 @@ remd_status remd_exchange_device(remd_handle h, const int* grids, long step, con
     du = h->d_u;
   }
   launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, step, du, seed, h->d_index,
-                    h->dT, h->dP, h->stream);
+                    h->dT, h->dP, h->d_step, h->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));   // host arrays (uoff) go out of scope
+  return REMD_OK;
+}
+
+remd_status remd_enable_device_exchange(remd_handle h, const int* grids, unsigned long long seed,
+                                        long long first_step) {
+  if (!h) return REMD_ERR_INVALID;
+  if (!grids) {
+    h->exch_enabled = false;
+    return REMD_OK;
+  }
+  for (int e = 0; e < h->nens; e++)
+    if (grids[2 * e] < 1 || grids[2 * e + 1] < 1 || grids[2 * e] * grids[2 * e + 1] != h->ens_nrep[e]) {
+      set_error("exchange grid does not match the replica count of ensemble " + std::to_string(e));
+      return REMD_ERR_INVALID;
+    }
+  std::vector<long long> st(h->nens, first_step);
+  CK(cudaMemcpyAsync(h->d_grid, grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_step, st.data(), h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->exch_enabled = true;
+  h->exch_seed = seed;
   return REMD_OK;
 }
 

@@ -1010,11 +1010,19 @@ __device__ inline double philox_uniform(unsigned long long seed, long step, int 
 
 // REMD::ReplicaExchange + ExchangeList (src/remd.cxx:467-538, src/remdinfo.cxx:54-125),
 // one thread per ensemble; pot/vol from the averages of the last interval.
+// step < 0: the ensemble's own interval counter (step_ctr[e]) is used and then
+// advanced, and the uniforms come from Philox -- the form captured in the
+// interval graph.
 __global__ void k_exchange(DevPtrs d, const int* grid, const int* rep_off, const int* u_off,
-                           int nens, long step, const double* u, unsigned long long seed,
-                           int* index, double* T, double* P) {
+                           int nens, long step_arg, const double* u, unsigned long long seed,
+                           int* index, double* T, double* P, long long* step_ctr) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nens) return;
+  long step = step_arg;
+  if (step_arg < 0) {
+    step = (long)step_ctr[e];
+    step_ctr[e] = step + 1;
+  }
   const int nt = grid[2 * e], np = grid[2 * e + 1];
   const int off = rep_off[e];
   const int pcon = d.rc[off].pconstant;
@@ -1138,8 +1146,9 @@ void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s) {
 }
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, unsigned long long seed, int* index,
-                       double* T, double* P, cudaStream_t s) {
-  k_exchange<<<(nens + 63) / 64, 64, 0, s>>>(d, grid, rep_off, u_off, nens, step, u, seed, index, T, P);
+                       double* T, double* P, long long* step_ctr, cudaStream_t s) {
+  k_exchange<<<(nens + 63) / 64, 64, 0, s>>>(d, grid, rep_off, u_off, nens, step, u, seed, index, T,
+                                             P, step_ctr);
 }
 
 }  // namespace remd

@@ -33,7 +33,7 @@ void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, unsigned long long seed, int* index,
-                       double* T, double* P, cudaStream_t s);
+                       double* T, double* P, long long* step_ctr, cudaStream_t s);
 int pack_stride(int nsite, int prec);
 int measure_fp32_fma(int device, double* ms, long long* flops);
 

@@ -105,6 +105,7 @@ def lib():
         L.remd_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.remd_exchange_device.argtypes = [C.c_void_p, _ip, C.c_long, _dp, C.c_ulonglong]
         L.remd_get_conditions.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        L.remd_enable_device_exchange.argtypes = [C.c_void_p, _ip, C.c_ulonglong, C.c_longlong]
         L.remd_write_chk.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         L.remd_wall_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, _dp]
@@ -276,6 +277,14 @@ class REMDGPU:
         g = np.ascontiguousarray(grids, dtype=np.int32).reshape(-1)
         up = _p(np.ascontiguousarray(u, dtype=np.float64)) if u is not None else None
         _check(lib().remd_exchange_device(self.h, _p(g, _ip), step, up, seed))
+
+    def enable_device_exchange(self, grids, seed=0, first_step=0):
+        """Run the Metropolis exchange on the device after every interval."""
+        if grids is None:
+            _check(lib().remd_enable_device_exchange(self.h, None, 0, 0))
+            return
+        g = np.ascontiguousarray(grids, dtype=np.int32).reshape(-1)
+        _check(lib().remd_enable_device_exchange(self.h, _p(g, _ip), seed, first_step))
 
     def execute_device(self):
         _check(lib().remd_execute_steps_device(self.h))

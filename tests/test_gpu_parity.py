@@ -288,3 +288,27 @@ def test_fp32_accuracy_tip5p_bulk_1728():
     assert rel(g["f"], orc.f) < 1e-5
     assert rel(g["n"], orc.n) < 1e-5
     assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
+
+
+def test_graph_exchange_equals_explicit_exchange():
+    """The exchange appended to the interval graph (device step counter, Philox
+    uniforms) makes the same decisions as explicit per-interval calls."""
+    ens = [S.small_ensemble("tip4p", 0, nmol=64, ntemp=4, npress=2, seed=51, interval=5),
+           S.small_ensemble("tip5p", 1, nmol=72, ntemp=2, npress=2, seed=52, interval=5)]
+    grids = [(e.ntemp, e.npress) for e in ens]
+    a = E.REMDGPU(ens, precision="fp32")
+    b = E.REMDGPU(ens, precision="fp32")
+    a.enable_device_exchange(grids, seed=99)
+    for step in range(8):
+        a.execute_device()
+        b.execute_device()
+        b.exchange_device(grids, step, u=None, seed=99)
+    ia, Ta, Pa = a.conditions()
+    ib, Tb, Pb = b.conditions()
+    assert np.array_equal(ia, ib) and np.array_equal(Ta, Tb) and np.array_equal(Pa, Pb)
+    assert np.array_equal(a.all_averages(), b.all_averages())
+    off = 0
+    for e in ens:      # conditions stay a permutation within each ensemble
+        assert sorted(ia[off:off + e.nreplica]) == list(range(e.nreplica))
+        assert np.array_equal(np.sort(Ta[off:off + e.nreplica]), np.sort(e.T))
+        off += e.nreplica
