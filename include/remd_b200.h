@@ -243,6 +243,29 @@ remd_status remd_read_chk(const char *path, int nmol, double *r, double *v, doub
 /* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) of replica rep. */
 remd_status remd_write_chk(remd_handle h, int rep, const char *path);
 
+/* Force snapshot of one replica that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory -- a host
+ * program whose own allocator already owns the GPU (an ML framework's caching
+ * allocator, a plugin host), or a loop that must not stall on cudaMalloc /
+ * cudaFree, which can synchronise the device.  The caller passes device
+ * buffers: d_r (nmol*3 box fractions), d_q (nmol*4 quaternions), d_wall (the
+ * nfwall x {f,U} table from remd_wall_table, 16-byte aligned; NULL for bulk),
+ * and receives d_f (nmol*3 forces), d_n (nmol*4 body torques) and d_out[8] =
+ * {LJ, Coulomb, wall, virial x3, unordered pairs within rcut, error word (0 ok,
+ * 1 neighbour overflow)}; L is the host box.  Same FP32 arithmetic as a
+ * REMD_PREC_FP32 handle's remd_compute_forces.  All working memory is one
+ * fixed device array of the library (about 5.6 MB, held by every GPU that
+ * loads it until exit): at most 2048 molecules and 1024 neighbours per molecule
+ * (rcut <= ~12.4 A); larger inputs are rejected with REMD_ERR_INVALID.  The
+ * first call on a device looks up that array's device address (set-up), so make
+ * it before any stream capture.  Calls share the array and keep the previous
+ * call's contents, so calls that overlap on the GPU (other streams, other
+ * threads) race; serialise them.  Asynchronous on `stream` (a cudaStream_t,
+ * NULL = default stream). */
+remd_status remd_force_snapshot_noalloc(const remd_system_desc *sys, const double *d_r,
+                                        const double *d_q, const double L[3], const double *d_wall,
+                                        double *d_f, double *d_n, double *d_out, void *stream);
+
 /* Text of the last error on this thread. */
 const char *remd_last_error(void);
 /* Library version string. */

@@ -1111,6 +1111,62 @@ int measure_fp32_fma(int device, double* ms, long long* flops) {
   return 0;
 }
 
+// ------------------------------------------------------------------ caller-buffer variant
+// Entry and exit kernels of remd_force_snapshot_noalloc (noalloc.cu): the
+// caller's AoS positions/quaternions into the scratch SoA arrays and force
+// records, and the scratch results back into the caller's AoS outputs.
+__global__ void k_noalloc_load(DevPtrs d, const double* __restrict__ r_aos,
+                               const double* __restrict__ q_aos) {
+  const Tile t = d.tiles[blockIdx.x];
+  const RepConst& c = d.rc[t.rep];
+  const int i = threadIdx.x;
+  if (i < t.count) {
+    const int li = t.start + i;
+    const int g = c.mol_off + li;
+    double r[3], q[4];
+    for (int x = 0; x < 3; x++) r[x] = r_aos[3 * li + x];
+    for (int x = 0; x < 4; x++) q[x] = q_aos[4 * li + x];
+    for (int x = 0; x < 3; x++) d.r[x * d.N + g] = r[x];
+    for (int x = 0; x < 4; x++) d.q[x * d.N + g] = q[x];
+    write_pack(d, c, kF32, li, r, q);
+  }
+  if (i == 0) {
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    d.Lbuild[3 * blockIdx.x] = nan;
+    if (blockIdx.x == 0) { *d.err = 0; d.status[0] = 0; }
+  }
+}
+
+// out: lj, clmb, wall, vir[3] (halved like ForceCalculator::Switching), the
+// number of unordered pairs within rcut, and the error word (0 = ok).
+__global__ void k_noalloc_store(DevPtrs d, double* __restrict__ f_aos, double* __restrict__ n_aos,
+                                double* __restrict__ out) {
+  const RepConst& c = d.rc[0];
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    for (int x = 0; x < 3; x++) f_aos[3 * li + x] = d.f[x * d.N + g];
+    for (int x = 0; x < 4; x++) n_aos[4 * li + x] = d.n[x * d.N + g];
+  }
+  if (threadIdx.x == 0) {
+    double lj, clmb, wall, vir[3];
+    reduce_part2(d, c, lj, clmb, wall, vir);
+    long long np = 0;
+    for (int t = c.tile_off; t < c.tile_off + c.ntile; t++) np += d.part2[t].npairs;
+    out[0] = lj; out[1] = clmb; out[2] = wall;
+    out[3] = vir[0]; out[4] = vir[1]; out[5] = vir[2];
+    out[6] = (double)(np / 2);
+    out[7] = (double)*d.err;
+  }
+}
+
+void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
+                         cudaStream_t s) {
+  k_noalloc_load<<<d.ntiles, tile, 0, s>>>(d, r_aos, q_aos);
+}
+void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s) {
+  k_noalloc_store<<<1, 256, 0, s>>>(d, f_aos, n_aos, out);
+}
+
 // ------------------------------------------------------------------ launchers
 void launch_pack(const DevPtrs& d, int prec, int tile, cudaStream_t s) {
   k_pack<<<d.ntiles, tile, 0, s>>>(d, prec);

@@ -35,6 +35,9 @@ void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, co
                        int nens, long step, const double* u, unsigned long long seed, int* index,
                        double* T, double* P, long long* step_ctr, cudaStream_t s);
 int pack_stride(int nsite, int prec);
+void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
+                         cudaStream_t s);
+void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s);
 int measure_fp32_fma(int device, double* ms, long long* flops);
 
 }  // namespace remd

@@ -106,6 +106,9 @@ def lib():
         L.remd_exchange_device.argtypes = [C.c_void_p, _ip, C.c_long, _dp, C.c_ulonglong]
         L.remd_get_conditions.argtypes = [C.c_void_p, _ip, _dp, _dp]
         L.remd_enable_device_exchange.argtypes = [C.c_void_p, _ip, C.c_ulonglong, C.c_longlong]
+        L.remd_force_snapshot_noalloc.argtypes = [C.POINTER(SystemDesc), C.c_void_p, C.c_void_p, _dp,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p]
         L.remd_write_chk.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
         L.remd_wall_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, _dp]
@@ -297,6 +300,16 @@ class REMDGPU:
 
     def write_chk(self, rep, path):
         _check(lib().remd_write_chk(self.h, rep, path.encode()))
+
+
+def force_snapshot_noalloc(spec, d_r, d_q, L, d_wall, d_f, d_n, d_out, stream=None):
+    """remd_force_snapshot_noalloc on caller-owned device buffers (addresses as
+    ints): for callers that cannot let the library allocate device memory.
+    Asynchronous on `stream` (a cudaStream_t as int, None = default stream)."""
+    d = system_desc(spec)
+    Lh = np.ascontiguousarray(L, dtype=np.float64)
+    _check(lib().remd_force_snapshot_noalloc(C.byref(d), d_r, d_q, _p(Lh), d_wall or None, d_f, d_n,
+                                             d_out, stream))
 
 
 def wall_table(confined, nfwall, wall_length, sgm, eps, rho):
