@@ -6,6 +6,7 @@
 // usage: shim_check <inp file> <chk file> <intervals>
 // prints one line per replica and interval: "rep <r> <k> gpu <19 averages> cpu <19 averages>"
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <vector>
 
@@ -43,7 +44,9 @@ int main(int argc, char** argv) {
   std::ifstream f(argv[1]);
   prm.read(f);
   const int nrep = prm.nreplica, nint = std::atoi(argv[3]);
-  REMDInfo info(prm);
+  // REMDInfo's destructor deletes its Histogram objects with delete[]
+  // (src/remdinfo.cxx:296-300): keep it alive until the process ends.
+  REMDInfo& info = *new REMDInfo(prm);
   std::vector<Molecules*> gpu(nrep), cpu(nrep);
   for (int k = 0; k < nrep; k++) {
     for (Molecules** mm : {&gpu[k], &cpu[k]}) {
@@ -73,5 +76,6 @@ int main(int argc, char** argv) {
   }
   eng.ConvertVariablesToHost(gpu.data());
   std::printf("state L %.17g %.17g %.17g s %.17g\n", gpu[0]->L[0], gpu[0]->L[1], gpu[0]->L[2], gpu[0]->tst->s);
-  return 0;
+  std::fflush(stdout);
+  std::_Exit(0);   // the reference's destructors free memory they never allocated
 }
