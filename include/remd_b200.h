@@ -312,6 +312,8 @@ remd_status remd_job_result(remd_server s, remd_job_id id, double *averages, int
  * of jobs still queued or running in *pending. */
 remd_status remd_server_step(remd_server s, int *pending);
 remd_status remd_server_stats_get(remd_server s, remd_server_stats *out);
+/* The device footprint the server budgets for a job (the engine's layout formula). */
+remd_status remd_job_bytes(const remd_job_desc *job, size_t *bytes);
 
 #ifdef __cplusplus
 }

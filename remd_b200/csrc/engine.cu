@@ -54,6 +54,7 @@ struct remd_engine_s {
   bool exch_enabled = false;        // device exchange appended to every interval
   unsigned long long exch_seed = 0;
   long long* d_step = nullptr;      // per-ensemble interval counter of the device exchange
+  unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
   long long last_pairs = 0;
   size_t bytes = 0;
 };
@@ -142,6 +143,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       (size_t)h->nens * 2 * 4, (size_t)h->nens * 4, (size_t)h->nens * 4,   // 24 grid 25 rep_off 26 u_off
       (size_t)std::max(nr / 2, (size_t)1) * 8,   // 27 u
       (size_t)h->nens * 8,             // 28 per-ensemble exchange step counter
+      (size_t)h->nens * 8,             // 29 per-ensemble exchange seed
   };
   offs.clear();
   total = 0;
@@ -200,6 +202,7 @@ static remd_status allocate(remd_engine_s* h) {
   h->d_u_off = reinterpret_cast<int*>(b + offs[26]);
   h->d_u = reinterpret_cast<double*>(b + offs[27]);
   h->d_step = reinterpret_cast<long long*>(b + offs[28]);
+  h->d_seed = reinterpret_cast<unsigned long long*>(b + offs[29]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
@@ -259,7 +262,7 @@ static remd_status build_graph(remd_engine_s* h) {
   }
   launch_replica_end(h->d, h->X, h->stream);
   if (h->exch_enabled)
-    launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, -1, nullptr, h->exch_seed,
+    launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, -1, nullptr, h->d_seed,
                       h->d_index, h->dT, h->dP, h->d_step, h->stream);
   cudaError_t le = cudaGetLastError();
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
@@ -286,6 +289,42 @@ static long long host_pairs(remd_engine_s* h) {
   for (auto& p : p2) s += p.npairs;
   return s / 2;
 }
+
+namespace remd {
+
+// ---- internals used by the serving loop (server.cu) ----
+remd_status engine_set_h0(remd_handle h, const double* H0) {
+  std::vector<RepState> st(h->nrep);
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(st.data(), h->X, st.size() * sizeof(RepState), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < h->nrep; k++) st[k].H0 = H0[k];
+  CK(cudaMemcpy(h->X, st.data(), st.size() * sizeof(RepState), cudaMemcpyHostToDevice));
+  return REMD_OK;
+}
+
+// Per-ensemble exchange set-up: grids (2 per ensemble), Philox seeds, next step,
+// and the condition-slot -> replica index (per replica, ensemble-local).
+remd_status engine_set_exchange(remd_handle h, const int* grids, const unsigned long long* seeds,
+                                const long long* steps, const int* index) {
+  CK(cudaMemcpyAsync(h->d_grid, grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_seed, seeds, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_step, steps, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_index, index, h->nrep * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->exch_enabled = true;
+  return REMD_OK;
+}
+
+remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(steps, h->d_step, h->nens * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(index, h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
+
+}  // namespace remd
 
 extern "C" {
 
@@ -742,7 +781,12 @@ remd_status remd_exchange_device(remd_handle h, const int* grids, long step, con
     if (tot > 0) CK(cudaMemcpyAsync(h->d_u, u, tot * 8, cudaMemcpyHostToDevice, h->stream));
     du = h->d_u;
   }
-  launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, step, du, seed, h->d_index,
+  {
+    std::vector<unsigned long long> sd(h->nens, seed);
+    CK(cudaMemcpyAsync(h->d_seed, sd.data(), h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, step, du, h->d_seed, h->d_index,
                     h->dT, h->dP, h->d_step, h->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));   // host arrays (uoff) go out of scope
@@ -762,8 +806,10 @@ remd_status remd_enable_device_exchange(remd_handle h, const int* grids, unsigne
       return REMD_ERR_INVALID;
     }
   std::vector<long long> st(h->nens, first_step);
+  std::vector<unsigned long long> sd(h->nens, seed);
   CK(cudaMemcpyAsync(h->d_grid, grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->d_step, st.data(), h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_seed, sd.data(), h->nens * 8, cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->exch_enabled = true;
   h->exch_seed = seed;

@@ -305,8 +305,9 @@ struct IAcc {
 };
 
 // FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU
-// plus one Newton step), partial sums in FP32 over at most 4 neighbours, then
-// FP64 accumulation.
+// plus one Newton step), partial sums in FP32 over 4 pairs within rcut, then
+// FP64 accumulation.  Lists are in ascending j, so the result depends only on
+// the positions (not on when the list was built).
 // SIMG: apply the minimum image to every site pair as the reference does
 // (src/force_calculator.cxx:737-741).  It changes the result only when a box
 // length is below 2 (rc + 2 site_reach); the caller enables it just then.
@@ -444,8 +445,10 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
       fv[2] += (fpz + cz) * dz;
       flj += sw * elj;
       fcl += sw * ecl;
+      // partial sums close every 4 pairs within rcut (not every 4 list entries),
+      // so the force is a function of the positions alone, whatever the list holds
+      if ((np & 3) == 0) { flush(); zero(); }
     }
-    if ((k & 3) == 3) { flush(); zero(); }
   }
   flush();
   a.npair += np;
@@ -1014,7 +1017,7 @@ __device__ inline double philox_uniform(unsigned long long seed, long step, int 
 // advanced, and the uniforms come from Philox -- the form captured in the
 // interval graph.
 __global__ void k_exchange(DevPtrs d, const int* grid, const int* rep_off, const int* u_off,
-                           int nens, long step_arg, const double* u, unsigned long long seed,
+                           int nens, long step_arg, const double* u, const unsigned long long* seeds,
                            int* index, double* T, double* P, long long* step_ctr) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nens) return;
@@ -1041,7 +1044,7 @@ __global__ void k_exchange(DevPtrs d, const int* grid, const int* rep_off, const
     const double b1 = 1. / Te[i1], b2 = 1. / Te[i2];
     double delta = (b2 - b1) * (pot_of(i1) - pot_of(i2));
     if (pcon > 0) delta += (b2 * Pe[i2] - b1 * Pe[i1]) * (vol_of(i1) - vol_of(i2));
-    const double uu = u ? u[u_off[e] + pair] : philox_uniform(seed, step, e, pair);
+    const double uu = u ? u[u_off[e] + pair] : philox_uniform(seeds[e], step, 0, pair);
     pair++;
     if (exp(-delta) > uu) {
       double t = Te[idx[a]]; Te[idx[a]] = Te[idx[b]]; Te[idx[b]] = t;
@@ -1201,9 +1204,9 @@ void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s) {
   k_replica_rescale<<<d.nrep, kRepThreads, 0, s>>>(d, X);
 }
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
-                       int nens, long step, const double* u, unsigned long long seed, int* index,
-                       double* T, double* P, long long* step_ctr, cudaStream_t s) {
-  k_exchange<<<(nens + 63) / 64, 64, 0, s>>>(d, grid, rep_off, u_off, nens, step, u, seed, index, T,
+                       int nens, long step, const double* u, const unsigned long long* seeds,
+                       int* index, double* T, double* P, long long* step_ctr, cudaStream_t s) {
+  k_exchange<<<(nens + 63) / 64, 64, 0, s>>>(d, grid, rep_off, u_off, nens, step, u, seeds, index, T,
                                              P, step_ctr);
 }
 

@@ -32,8 +32,8 @@ void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
-                       int nens, long step, const double* u, unsigned long long seed, int* index,
-                       double* T, double* P, long long* step_ctr, cudaStream_t s);
+                       int nens, long step, const double* u, const unsigned long long* seeds,
+                       int* index, double* T, double* P, long long* step_ctr, cudaStream_t s);
 int pack_stride(int nsite, int prec);
 void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
                          cudaStream_t s);

@@ -1,0 +1,430 @@
+// server.cu -- continuous batching of REMD jobs on one GPU.
+//
+// A job is one REMD system (an ensemble: ntemp x npress replicas) to be run for
+// `ninterval` intervals (MD + Metropolis exchange each).  remd_server_step()
+// is one scheduling round:
+//   1. finished and cancelled jobs leave the batch, freeing their HBM;
+//   2. queued jobs are admitted in arrival order while their estimated device
+//      footprint fits the budget (and their interval matches the batch's);
+//   3. if the batch changed, the running jobs' states are pulled from the
+//      device and one engine handle is built for the new set (state, H0,
+//      exchange index, step counter and seed carried over exactly);
+//   4. every job in the batch advances one interval in one graph launch.
+// Forces are a pure function of the positions (see pair_loop_f32) and every
+// per-replica reduction has a fixed order, so a job's trajectory is the same
+// bit for bit whether it runs alone or with any batch mates, and across batch
+// rebuilds (tests/test_gpu_server.py).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/remd_b200.h"
+#include "hostio.h"
+
+namespace remd {
+remd_status engine_set_h0(remd_handle h, const double* H0);
+remd_status engine_set_exchange(remd_handle h, const int* grids, const unsigned long long* seeds,
+                                const long long* steps, const int* index);
+remd_status engine_get_exchange(remd_handle h, long long* steps, int* index);
+size_t engine_bytes(remd_handle h);
+}  // namespace remd
+
+using namespace remd;
+
+namespace {
+
+struct Rep {
+  std::vector<double> r, v, q, p, m, I;
+  double s, Ps, Q, Pv[3], W, L[3], T, P, H0;
+  bool has_h0 = false;
+};
+
+struct Job {
+  remd_job_id id;
+  remd_system_desc sys;
+  int nt, np;
+  int ninterval, done = 0;
+  unsigned long long seed;
+  int state = 0;   // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
+  remd_status status = REMD_OK;
+  double t_submit = 0, t_start = 0, t_end = 0;
+  std::vector<Rep> reps;
+  std::vector<int> index;          // condition slot -> replica
+  long long step = 0;              // next exchange list type = step % 4
+  std::vector<double> avg;         // latest averages, nrep x 19
+  size_t bytes = 0;
+  int nrep() const { return nt * np; }
+};
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// Device footprint of a job, with the engine's own layout formula.
+size_t estimate_bytes(const remd_system_desc& s, int nrep) {
+  const double rl = s.rcut + 1.0;
+  int cap = ((int)std::ceil(0.1 * 4.0 / 3.0 * M_PI * rl * rl * rl) + 7) / 8 * 8;
+  cap = std::min(cap, s.nmol - 1);
+  const size_t ntile = (s.nmol + 127) / 128;
+  const size_t per_rep = (size_t)s.nmol * (176 + 80 + 16 + 4) + ntile * (size_t)cap * 128 * 2 +
+                         ntile * (3 * 8 + 64 + 64 + 16) + 1024;
+  return per_rep * nrep + (size_t)std::max(s.nfwall, 0) * 16 + 4096;
+}
+
+double pct(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double x = q * (v.size() - 1);
+  const size_t i = (size_t)x;
+  const double f = x - i;
+  return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+struct remd_server_s {
+  std::mutex mu;
+  size_t budget = 0;
+  int device = 0;
+  remd_precision prec = REMD_PREC_FP32;
+  remd_job_id next_id = 1;
+  std::vector<Job*> jobs;          // every job ever submitted (owned)
+  std::vector<Job*> queue;         // waiting, in arrival order
+  std::vector<Job*> active;        // in the current batch, in batch order
+  remd_handle batch = nullptr;
+  bool dirty = false;
+  size_t in_use = 0;
+  double t0 = now_s();
+  std::vector<double> interval_ms, job_s;
+  long long jobs_done = 0, intervals_done = 0, mol_steps = 0;
+  double busy_s = 0.0;
+
+  Job* find(remd_job_id id) {
+    for (Job* j : jobs)
+      if (j->id == id) return j;
+    return nullptr;
+  }
+};
+
+static remd_status pull_batch(remd_server_s* S) {
+  if (!S->batch) return REMD_OK;
+  int nens = (int)S->active.size();
+  std::vector<long long> steps(nens);
+  int total = 0;
+  for (Job* j : S->active) total += j->nrep();
+  std::vector<int> idx(total);
+  remd_status st = engine_get_exchange(S->batch, steps.data(), idx.data());
+  if (st != REMD_OK) return st;
+  int rep = 0;
+  for (int e = 0; e < nens; e++) {
+    Job* j = S->active[e];
+    j->step = steps[e];
+    for (int k = 0; k < j->nrep(); k++, rep++) {
+      Rep& R = j->reps[k];
+      j->index[k] = idx[rep];
+      remd_state_view sv{};
+      sv.r = R.r.data(); sv.v = R.v.data(); sv.q = R.q.data(); sv.p = R.p.data();
+      if ((st = remd_get_state(S->batch, rep, &sv)) != REMD_OK) return st;
+      R.s = sv.s; R.Ps = sv.Ps;
+      for (int x = 0; x < 3; x++) { R.Pv[x] = sv.Pv[x]; R.L[x] = sv.L[x]; }
+      R.H0 = sv.H0;
+      R.has_h0 = true;
+    }
+  }
+  // the device conditions (after the last exchange) become the replicas' T, P
+  std::vector<double> T(total), P(total);
+  if ((st = remd_get_conditions(S->batch, nullptr, T.data(), P.data())) != REMD_OK) return st;
+  rep = 0;
+  for (Job* j : S->active)
+    for (int k = 0; k < j->nrep(); k++, rep++) { j->reps[k].T = T[rep]; j->reps[k].P = P[rep]; }
+  return REMD_OK;
+}
+
+static remd_status build_batch(remd_server_s* S) {
+  if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
+  if (S->active.empty()) return REMD_OK;
+  std::vector<remd_system_desc> sys;
+  std::vector<int> per;
+  std::vector<remd_replica_init> init;
+  std::vector<int> grids, index;
+  std::vector<unsigned long long> seeds;
+  std::vector<long long> steps;
+  std::vector<double> H0;
+  bool any_h0 = false;
+  for (Job* j : S->active) {
+    sys.push_back(j->sys);
+    per.push_back(j->nrep());
+    grids.push_back(j->nt);
+    grids.push_back(j->np);
+    seeds.push_back(j->seed);
+    steps.push_back(j->step);
+    for (int k = 0; k < j->nrep(); k++) {
+      const Rep& R = j->reps[k];
+      remd_replica_init ri{};
+      ri.r = R.r.data(); ri.v = R.v.data(); ri.q = R.q.data(); ri.p = R.p.data();
+      ri.mass = R.m.data(); ri.inertia = R.I.data();
+      ri.s = R.s; ri.Ps = R.Ps; ri.Q = R.Q; ri.W = R.W; ri.T = R.T; ri.P = R.P;
+      for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
+      init.push_back(ri);
+      index.push_back(j->index[k]);
+      H0.push_back(R.H0);
+      any_h0 = any_h0 || R.has_h0;
+    }
+  }
+  remd_status st = remd_create(sys.data(), (int)sys.size(), per.data(), init.data(), S->prec, S->device,
+                               &S->batch);
+  if (st != REMD_OK) return st;
+  if (any_h0) {
+    // a running job keeps its Hamiltonian reference; a new one takes the fresh value
+    std::vector<double> fresh(init.size());
+    int rep = 0;
+    for (Job* j : S->active)
+      for (int k = 0; k < j->nrep(); k++, rep++) {
+        remd_state_view sv{};
+        if ((st = remd_get_state(S->batch, rep, &sv)) != REMD_OK) return st;
+        fresh[rep] = j->reps[k].has_h0 ? j->reps[k].H0 : sv.H0;
+      }
+    if ((st = engine_set_h0(S->batch, fresh.data())) != REMD_OK) return st;
+  }
+  return engine_set_exchange(S->batch, grids.data(), seeds.data(), steps.data(), index.data());
+}
+
+extern "C" {
+
+remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision prec,
+                             remd_server* out) {
+  if (!out || hbm_budget_bytes == 0) {
+    set_error("remd_server_open: need an output handle and a budget > 0");
+    return REMD_ERR_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    set_error("no CUDA device");
+    return REMD_ERR_NO_DEVICE;
+  }
+  auto* S = new remd_server_s;
+  S->budget = hbm_budget_bytes;
+  S->device = device;
+  S->prec = prec;
+  *out = S;
+  return REMD_OK;
+}
+
+remd_status remd_server_close(remd_server S) {
+  if (!S) return REMD_OK;
+  if (S->batch) remd_destroy(S->batch);
+  for (Job* j : S->jobs) delete j;
+  delete S;
+  return REMD_OK;
+}
+
+remd_status remd_job_submit(remd_server S, const remd_job_desc* jd, remd_job_id* id) {
+  if (!S || !jd || !id || !jd->reps || jd->ntemp < 1 || jd->npress < 1 || jd->ninterval < 1 ||
+      jd->system.nmol < 2) {
+    set_error("remd_job_submit: bad job description");
+    return REMD_ERR_INVALID;
+  }
+  auto* j = new Job;
+  j->sys = jd->system;
+  j->nt = jd->ntemp;
+  j->np = jd->npress;
+  j->ninterval = jd->ninterval;
+  j->seed = jd->seed;
+  const int n = jd->system.nmol;
+  for (int k = 0; k < j->nrep(); k++) {
+    const remd_replica_init& ri = jd->reps[k];
+    if (!ri.r || !ri.v || !ri.q || !ri.p || !ri.mass || !ri.inertia) {
+      delete j;
+      set_error("remd_job_submit: null state array");
+      return REMD_ERR_INVALID;
+    }
+    Rep R;
+    R.r.assign(ri.r, ri.r + 3 * n); R.v.assign(ri.v, ri.v + 3 * n);
+    R.q.assign(ri.q, ri.q + 4 * n); R.p.assign(ri.p, ri.p + 4 * n);
+    R.m.assign(ri.mass, ri.mass + n); R.I.assign(ri.inertia, ri.inertia + 3 * n);
+    R.s = ri.s; R.Ps = ri.Ps; R.Q = ri.Q; R.W = ri.W; R.T = ri.T; R.P = ri.P; R.H0 = 0.0;
+    for (int x = 0; x < 3; x++) { R.Pv[x] = ri.Pv[x]; R.L[x] = ri.L[x]; }
+    j->reps.push_back(R);
+    j->index.push_back(k);
+  }
+  j->bytes = estimate_bytes(j->sys, j->nrep());
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (j->bytes > S->budget) {
+    delete j;
+    set_error("remd_job_submit: the job alone exceeds the HBM budget");
+    return REMD_ERR_OOM;
+  }
+  j->id = S->next_id++;
+  j->t_submit = now_s() - S->t0;
+  S->jobs.push_back(j);
+  S->queue.push_back(j);
+  *id = j->id;
+  return REMD_OK;
+}
+
+remd_status remd_job_poll(remd_server S, remd_job_id id, remd_job_info* info) {
+  if (!S || !info) return REMD_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  Job* j = S->find(id);
+  if (!j) { set_error("unknown job"); return REMD_ERR_INVALID; }
+  info->state = j->state;
+  info->intervals_done = j->done;
+  info->submit_s = j->t_submit;
+  info->start_s = j->t_start;
+  info->end_s = j->t_end;
+  info->status = j->status;
+  return REMD_OK;
+}
+
+remd_status remd_job_cancel(remd_server S, remd_job_id id) {
+  if (!S) return REMD_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  Job* j = S->find(id);
+  if (!j) { set_error("unknown job"); return REMD_ERR_INVALID; }
+  if (j->state == 0) {
+    S->queue.erase(std::find(S->queue.begin(), S->queue.end(), j));
+    j->state = 4;
+    j->status = REMD_ERR_CANCELLED;
+    j->t_end = now_s() - S->t0;
+  } else if (j->state == 1) {
+    j->state = 4;   // leaves the batch at the next scheduling round
+    j->status = REMD_ERR_CANCELLED;
+  }
+  return REMD_OK;
+}
+
+remd_status remd_job_result(remd_server S, remd_job_id id, double* averages, int* index) {
+  if (!S) return REMD_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  Job* j = S->find(id);
+  if (!j) { set_error("unknown job"); return REMD_ERR_INVALID; }
+  if (j->state != 2) { set_error("job not finished"); return REMD_ERR_INVALID; }
+  if (averages) std::memcpy(averages, j->avg.data(), j->avg.size() * 8);
+  if (index) std::memcpy(index, j->index.data(), j->index.size() * 4);
+  return REMD_OK;
+}
+
+remd_status remd_server_step(remd_server S, int* pending) {
+  if (!S) return REMD_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  // 1. leave: cancelled jobs (finished ones left at the end of their last round)
+  for (size_t e = 0; e < S->active.size();) {
+    Job* j = S->active[e];
+    if (j->state == 4) {
+      if (!S->dirty) {
+        remd_status st = pull_batch(S);
+        if (st != REMD_OK) return st;
+      }
+      S->dirty = true;
+      S->in_use -= j->bytes;
+      j->t_end = now_s() - S->t0;
+      S->active.erase(S->active.begin() + e);
+    } else {
+      e++;
+    }
+  }
+  // 2. admit in arrival order while the budget allows
+  while (!S->queue.empty()) {
+    Job* j = S->queue.front();
+    if (!S->active.empty() && j->sys.interval != S->active[0]->sys.interval) break;
+    if (S->in_use + j->bytes > S->budget) break;
+    if (!S->dirty && S->batch) {
+      remd_status st = pull_batch(S);
+      if (st != REMD_OK) return st;
+    }
+    S->queue.erase(S->queue.begin());
+    S->active.push_back(j);
+    S->in_use += j->bytes;
+    j->state = 1;
+    j->t_start = now_s() - S->t0;
+    S->dirty = true;
+  }
+  // 3. rebuild the batch handle if its membership changed
+  if (S->dirty) {
+    remd_status st = build_batch(S);
+    if (st != REMD_OK) {
+      for (Job* j : S->active) { j->state = 3; j->status = st; }
+      S->active.clear();
+      S->in_use = 0;
+      S->dirty = false;
+      return st;
+    }
+    S->dirty = false;
+  }
+  // 4. one interval (MD + exchange) for every running job
+  if (S->batch) {
+    const double t0 = now_s();
+    remd_status st = remd_execute_steps_device(S->batch);
+    const double dt = now_s() - t0;
+    S->interval_ms.push_back(dt * 1e3);
+    S->busy_s += dt;
+    S->intervals_done++;
+    int total = 0;
+    for (Job* j : S->active) total += j->nrep();
+    std::vector<double> avg((size_t)total * 19);
+    if (st == REMD_OK) st = remd_get_all_averages(S->batch, avg.data());
+    int rep = 0;
+    bool left = false;
+    for (Job* j : S->active) {
+      j->avg.assign(avg.begin() + (size_t)rep * 19, avg.begin() + (size_t)(rep + j->nrep()) * 19);
+      rep += j->nrep();
+      if (st != REMD_OK) { j->state = 3; j->status = st; left = true; continue; }
+      j->done++;
+      S->mol_steps += (long long)j->sys.nmol * j->nrep() * j->sys.interval;
+      if (j->done >= j->ninterval) {
+        j->state = 2;
+        left = true;
+      }
+    }
+    if (left) {
+      remd_status pst = pull_batch(S);   // final index/state of leaving jobs, carry-over of the rest
+      if (pst != REMD_OK) return pst;
+      for (size_t e = 0; e < S->active.size();) {
+        Job* j = S->active[e];
+        if (j->state == 2 || j->state == 3) {
+          j->t_end = now_s() - S->t0;
+          if (j->state == 2) { S->job_s.push_back(j->t_end - j->t_submit); S->jobs_done++; }
+          S->in_use -= j->bytes;
+          S->active.erase(S->active.begin() + e);
+          S->dirty = true;
+        } else {
+          e++;
+        }
+      }
+    }
+    if (st != REMD_OK) return st;
+  }
+  if (pending) *pending = (int)(S->queue.size() + S->active.size());
+  return REMD_OK;
+}
+
+remd_status remd_job_bytes(const remd_job_desc* jd, size_t* out) {
+  if (!jd || !out || jd->ntemp < 1 || jd->npress < 1 || jd->system.nmol < 2) return REMD_ERR_INVALID;
+  *out = estimate_bytes(jd->system, jd->ntemp * jd->npress);
+  return REMD_OK;
+}
+
+remd_status remd_server_stats_get(remd_server S, remd_server_stats* o) {
+  if (!S || !o) return REMD_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(S->mu);
+  o->jobs_done = S->jobs_done;
+  o->intervals_done = S->intervals_done;
+  o->mol_steps = S->mol_steps;
+  o->p50_interval_ms = pct(S->interval_ms, 0.50);
+  o->p99_interval_ms = pct(S->interval_ms, 0.99);
+  o->p50_job_s = pct(S->job_s, 0.50);
+  o->p99_job_s = pct(S->job_s, 0.99);
+  o->busy_s = S->busy_s;
+  o->bytes_in_use = (long long)S->in_use;
+  o->budget_bytes = (long long)S->budget;
+  return REMD_OK;
+}
+
+}  // extern "C"

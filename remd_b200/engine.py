@@ -106,6 +106,15 @@ def lib():
         L.remd_exchange_device.argtypes = [C.c_void_p, _ip, C.c_long, _dp, C.c_ulonglong]
         L.remd_get_conditions.argtypes = [C.c_void_p, _ip, _dp, _dp]
         L.remd_enable_device_exchange.argtypes = [C.c_void_p, _ip, C.c_ulonglong, C.c_longlong]
+        L.remd_server_open.argtypes = [C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.remd_server_close.argtypes = [C.c_void_p]
+        L.remd_job_submit.argtypes = [C.c_void_p, C.POINTER(JobDesc), C.POINTER(C.c_longlong)]
+        L.remd_job_poll.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(JobInfo)]
+        L.remd_job_cancel.argtypes = [C.c_void_p, C.c_longlong]
+        L.remd_job_result.argtypes = [C.c_void_p, C.c_longlong, _dp, _ip]
+        L.remd_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        L.remd_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.remd_job_bytes.argtypes = [C.POINTER(JobDesc), C.POINTER(C.c_size_t)]
         L.remd_force_snapshot_noalloc.argtypes = [C.POINTER(SystemDesc), C.c_void_p, C.c_void_p, _dp,
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]
@@ -144,6 +153,110 @@ def system_desc(spec) -> SystemDesc:
     d.sgm_wall, d.eps_wall, d.rho_wall = spec.sgm_wall, spec.eps_wall, spec.rho_wall
     d.interval = spec.interval
     return d
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("system", SystemDesc), ("ntemp", C.c_int), ("npress", C.c_int),
+                ("reps", C.POINTER(ReplicaInit)), ("ninterval", C.c_int), ("seed", C.c_ulonglong)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("intervals_done", C.c_int), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("end_s", C.c_double), ("status", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_done", C.c_longlong), ("intervals_done", C.c_longlong),
+                ("mol_steps", C.c_longlong), ("p50_interval_ms", C.c_double),
+                ("p99_interval_ms", C.c_double), ("p50_job_s", C.c_double),
+                ("p99_job_s", C.c_double), ("busy_s", C.c_double),
+                ("bytes_in_use", C.c_longlong), ("budget_bytes", C.c_longlong)]
+
+
+def _replica_inits(states):
+    keep = []
+    inits = (ReplicaInit * len(states))()
+    for k, st in enumerate(states):
+        arrs = [np.ascontiguousarray(getattr(st, f), dtype=np.float64)
+                for f in ("r", "v", "q", "p", "m", "I")]
+        keep.append(arrs)
+        ri = inits[k]
+        ri.r, ri.v, ri.q, ri.p, ri.mass, ri.inertia = [_p(a) for a in arrs]
+        ri.s, ri.Ps, ri.Q, ri.W, ri.T, ri.P = st.s, st.Ps, st.Q, st.W, st.T, st.P
+        for x in range(3):
+            ri.Pv[x] = st.Pv[x]
+            ri.L[x] = st.L[x]
+    return inits, keep
+
+
+class Server:
+    """Continuous batching of REMD jobs (include/remd_b200.h, serving section)."""
+
+    def __init__(self, budget_bytes, precision="fp32", device=0):
+        self.h = C.c_void_p()
+        _check(lib().remd_server_open(C.c_size_t(int(budget_bytes)), device,
+                                      1 if precision == "fp64" else 0, C.byref(self.h)))
+
+    @staticmethod
+    def job_desc(ensemble, ninterval, seed=0, interval=None):
+        d = JobDesc()
+        d.system = system_desc(ensemble.spec)
+        if interval is not None:
+            d.system.interval = interval
+        d.ntemp, d.npress = ensemble.ntemp, ensemble.npress
+        inits, keep = _replica_inits(ensemble.states)
+        d.reps = inits
+        d.ninterval, d.seed = ninterval, seed
+        return d, (inits, keep)
+
+    @staticmethod
+    def job_bytes(ensemble):
+        d, keep = Server.job_desc(ensemble, 1)
+        out = C.c_size_t()
+        _check(lib().remd_job_bytes(C.byref(d), C.byref(out)))
+        return out.value
+
+    def submit(self, ensemble, ninterval, seed=0, interval=None):
+        d = JobDesc()
+        d.system = system_desc(ensemble.spec)
+        if interval is not None:
+            d.system.interval = interval
+        d.ntemp, d.npress = ensemble.ntemp, ensemble.npress
+        inits, keep = _replica_inits(ensemble.states)
+        d.reps = inits
+        d.ninterval, d.seed = ninterval, seed
+        jid = C.c_longlong()
+        _check(lib().remd_job_submit(self.h, C.byref(d), C.byref(jid)))
+        return jid.value
+
+    def step(self):
+        pending = C.c_int()
+        _check(lib().remd_server_step(self.h, C.byref(pending)))
+        return pending.value
+
+    def poll(self, jid):
+        info = JobInfo()
+        _check(lib().remd_job_poll(self.h, C.c_longlong(jid), C.byref(info)))
+        return info
+
+    def cancel(self, jid):
+        _check(lib().remd_job_cancel(self.h, C.c_longlong(jid)))
+
+    def result(self, jid, nrep):
+        avg = np.zeros((nrep, NUM_AVG))
+        idx = np.zeros(nrep, dtype=np.int32)
+        _check(lib().remd_job_result(self.h, C.c_longlong(jid), _p(avg), _p(idx, _ip)))
+        return avg, idx
+
+    def stats(self):
+        s = ServerStats()
+        _check(lib().remd_server_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().remd_server_close(self.h)
+            self.h = C.c_void_p()
 
 
 class REMDGPU:
