@@ -78,6 +78,11 @@ def workload(config, seed, interval):
     return ens
 
 
+def rank_workload(args, rank):
+    """Replicas only: every rank runs its own seeded copy of the workload."""
+    return workload(args.config, args.seed + 1000 * rank, args.interval)
+
+
 def workload_desc(config, ens, interval):
     n = [e.spec.nmol for e in ens for _ in e.states]
     name = {4: "uneven batch: 8 ensembles / 256 replicas, TIP3P/4P/5P, bulk+tube+slit",
@@ -106,24 +111,35 @@ def dist_setup(args):
     return rank, world, local
 
 
-def reduce_max(x, world):
+def _reduce(x, world, op):
+    """All-reduce one scalar (host plumbing for the bench line, not a data-path
+    collective): on the current CUDA device under NCCL, on the host under gloo."""
     if world == 1:
         return float(x)
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def reduce_max(x, world):
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.MAX)
 
 
 def reduce_sum(x, world):
-    if world == 1:
-        return float(x)
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, dist.ReduceOp.SUM)
+
+
+def aggregate(local_ms, local_units, world):
+    """Whole-job throughput of the replicas-only run: every rank's units over the
+    slowest rank's device time.  Returns (value, max_ms, total_units)."""
+    max_ms = reduce_max(local_ms, world)
+    total = reduce_sum(local_units, world)
+    return total / (max_ms * 1e-3), max_ms, total
 
 
 def barrier(world):
@@ -269,7 +285,7 @@ def engine_arm(args, rank, world, local):
     from remd_b200 import engine as E
     dev = local
     torch.cuda.set_device(dev)
-    ens = workload(args.config, args.seed + 1000 * rank, args.interval)
+    ens = rank_workload(args, rank)
     eng = E.REMDGPU(ens, precision="fp32", device=dev)
     if args.tile != 128 or args.skin != 1.0:
         eng.set_tuning(args.tile, args.skin)
@@ -307,9 +323,7 @@ def engine_arm(args, rank, world, local):
     clk = clocks.stop()
     ms = [a.elapsed_time(b) for a, b in evs]
     local_ms = float(sum(ms))
-    max_ms = reduce_max(local_ms, world)
-    total_units = reduce_sum(mol_steps_per_interval * args.steps, world)
-    value = total_units / (max_ms * 1e-3)
+    value, max_ms, total_units = aggregate(local_ms, mol_steps_per_interval * args.steps, world)
     statuses = [eng.replica_status(r) for r in range(eng.nrep)]
 
     # roofline of the force kernel: per-launch algorithmic FLOPs / event duration

@@ -322,6 +322,14 @@ remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
   return REMD_OK;
 }
 
+// Conditions to apply (with the exchange tail) at the start of the next interval.
+remd_status engine_set_pending_conditions(remd_handle h, const double* T, const double* P) {
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(h->dT, T, h->nrep * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->dP, P, h->nrep * 8, cudaMemcpyHostToDevice));
+  return REMD_OK;
+}
+
 size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
 
 }  // namespace remd

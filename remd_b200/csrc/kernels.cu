@@ -305,42 +305,43 @@ struct IAcc {
 };
 
 // FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU
-// plus one Newton step), partial sums in FP32 over 4 pairs within rcut, then
-// FP64 accumulation.  Lists are in ascending j, so the result depends only on
-// the positions (not on when the list was built).
+// plus one Newton step), partial sums in FP32 over 8 pairs within rcut, then
+// FP64 accumulation into this thread's slots of `acc` (shared memory, field f
+// at acc[f * blockDim.x + threadIdx.x]: 3S site-force components, 3 switching-
+// correction, 3 virial, LJ, Coulomb).  Lists are in ascending j, so the result
+// depends only on the positions (not on when the list was built).  The record
+// of neighbour k+1 is loaded while neighbour k is computed.
 // SIMG: apply the minimum image to every site pair as the reference does
 // (src/force_calculator.cxx:737-741).  It changes the result only when a box
 // length is below 2 (rc + 2 site_reach); the caller enables it just then.
+struct F32Const {
+  float qq[kMaxSites][kMaxSites];
+  float Ls[3], Lf[3], hL[3];
+};
+
 template <int S, int C0, bool SIMG>
-__device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
-                              const uint16_t* nb, int cnt, IAcc& a) {
+__device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const F32Const& k32,
+                              const uint16_t* nb, int cnt, double* acc, long long& npair) {
   constexpr int STRIDE = ((3 + 3 * S) + 3) / 4 * 4;
-  const int li = t.start + threadIdx.x;
-  const uint32_t* base = reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off;
-  uint32_t wi[STRIDE];
+  constexpr int NV = STRIDE / 4;
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int li = t.start + tid;
+  const uint4* base = reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off);
+  int xi, yi, zi;
+  float si[S][3];
   {
-    const uint4* p4 = reinterpret_cast<const uint4*>(base + (long long)li * STRIDE);
+    uint32_t wi[STRIDE];
 #pragma unroll
-    for (int k = 0; k < STRIDE / 4; k++) {
-      const uint4 u = __ldg(p4 + k);
+    for (int k = 0; k < NV; k++) {
+      const uint4 u = __ldg(base + (long long)li * NV + k);
       wi[4 * k] = u.x; wi[4 * k + 1] = u.y; wi[4 * k + 2] = u.z; wi[4 * k + 3] = u.w;
     }
+    xi = (int)wi[0]; yi = (int)wi[1]; zi = (int)wi[2];
+#pragma unroll
+    for (int k = 0; k < S; k++)
+#pragma unroll
+      for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
   }
-  const int xi = (int)wi[0], yi = (int)wi[1], zi = (int)wi[2];
-  float si[S][3];
-#pragma unroll
-  for (int k = 0; k < S; k++)
-#pragma unroll
-    for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
-  float qq[S][S];
-#pragma unroll
-  for (int k = 0; k < S; k++)
-#pragma unroll
-    for (int l = 0; l < S; l++) qq[k][l] = (float)c.qq[k][l];
-  const float Lsx = (float)(L[0] * kFixInv), Lsy = (float)(L[1] * kFixInv),
-              Lsz = (float)(L[2] * kFixInv);
-  const float Lfx = (float)L[0], Lfy = (float)L[1], Lfz = (float)L[2];
-  const float hLx = 0.5f * Lfx, hLy = 0.5f * Lfy, hLz = 0.5f * Lfz;
   const float rc = (float)c.rc, rs = (float)c.rs, rc2 = (float)(c.rc * c.rc);
   const float coef = (float)c.coef_sw;
   const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
@@ -357,26 +358,37 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 #pragma unroll
     for (int k = 0; k < S; k++)
 #pragma unroll
-      for (int x = 0; x < 3; x++) a.fs[k][x] += (double)fs[k][x];
+      for (int x = 0; x < 3; x++) acc[(3 * k + x) * T + tid] += (double)fs[k][x];
 #pragma unroll
-    for (int x = 0; x < 3; x++) { a.fc[x] += (double)fc[x]; a.vir[x] += (double)fv[x]; }
-    a.lj += (double)flj;
-    a.clmb += (double)fcl;
+    for (int x = 0; x < 3; x++) {
+      acc[(3 * S + x) * T + tid] += (double)fc[x];
+      acc[(3 * S + 3 + x) * T + tid] += (double)fv[x];
+    }
+    acc[(3 * S + 6) * T + tid] += (double)flj;
+    acc[(3 * S + 7) * T + tid] += (double)fcl;
   };
   zero();
   long long np = 0;
-  for (int k = 0; k < cnt; k++) {
-    const int j = nb[(long long)k * blockDim.x];
-    uint32_t wj[STRIDE];
-    const uint4* p4 = reinterpret_cast<const uint4*>(base + (long long)j * STRIDE);
+  uint4 nx[NV];
+  if (cnt > 0) {
+    const int j0 = nb[0];
 #pragma unroll
-    for (int m = 0; m < STRIDE / 4; m++) {
-      const uint4 u = __ldg(p4 + m);
-      wj[4 * m] = u.x; wj[4 * m + 1] = u.y; wj[4 * m + 2] = u.z; wj[4 * m + 3] = u.w;
+    for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)j0 * NV + m);
+  }
+  for (int k = 0; k < cnt; k++) {
+    uint32_t wj[STRIDE];
+#pragma unroll
+    for (int m = 0; m < NV; m++) {
+      wj[4 * m] = nx[m].x; wj[4 * m + 1] = nx[m].y; wj[4 * m + 2] = nx[m].z; wj[4 * m + 3] = nx[m].w;
     }
-    const float dx = (float)(int)(xi - (int)wj[0]) * Lsx;
-    const float dy = (float)(int)(yi - (int)wj[1]) * Lsy;
-    const float dz = (float)(int)(zi - (int)wj[2]) * Lsz;
+    if (k + 1 < cnt) {
+      const int jn = nb[(long long)(k + 1) * T];
+#pragma unroll
+      for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
+    }
+    const float dx = (float)(int)(xi - (int)wj[0]) * k32.Ls[0];
+    const float dy = (float)(int)(yi - (int)wj[1]) * k32.Ls[1];
+    const float dz = (float)(int)(zi - (int)wj[2]) * k32.Ls[2];
     const float r2 = dx * dx + dy * dy + dz * dz;
     if (r2 <= rc2) {
       np++;
@@ -388,11 +400,6 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
         sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
         dsw = coef * 30.f * r01c * r01c * r01l * r01l;
       }
-      float sj[S][3];
-#pragma unroll
-      for (int l = 0; l < S; l++)
-#pragma unroll
-        for (int x = 0; x < 3; x++) sj[l][x] = __uint_as_float(wj[3 + 3 * l + x]);
       float elj = 0.f, ecl = 0.f;
       float fpx = 0.f, fpy = 0.f, fpz = 0.f;
 #pragma unroll
@@ -405,14 +412,16 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
           const bool lj_pair = (kk == 0 && l == 0);
           const bool cl_pair = (kk >= C0 && l >= C0);
           if (!lj_pair && !cl_pair) continue;
-          float x = ax - sj[l][0], y = ay - sj[l][1], z = az - sj[l][2];
+          float x = ax - __uint_as_float(wj[3 + 3 * l]);
+          float y = ay - __uint_as_float(wj[3 + 3 * l + 1]);
+          float z = az - __uint_as_float(wj[3 + 3 * l + 2]);
           if (SIMG) {
-            if (x >= hLx) x -= Lfx;
-            if (x < -hLx) x += Lfx;
-            if (y >= hLy) y -= Lfy;
-            if (y < -hLy) y += Lfy;
-            if (z >= hLz) z -= Lfz;
-            if (z < -hLz) z += Lfz;
+            if (x >= k32.hL[0]) x -= k32.Lf[0];
+            if (x < -k32.hL[0]) x += k32.Lf[0];
+            if (y >= k32.hL[1]) y -= k32.Lf[1];
+            if (y < -k32.hL[1]) y += k32.Lf[1];
+            if (z >= k32.hL[2]) z -= k32.Lf[2];
+            if (z < -k32.hL[2]) z += k32.Lf[2];
           }
           const float rr = x * x + y * y + z * z;
           float ri = rsqrtf(rr);
@@ -426,7 +435,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
             ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
           }
           if (cl_pair) {
-            const float e = qq[kk][l] * ri;
+            const float e = k32.qq[kk][l] * ri;
             ecl += e;
             ftmp += e * ri2;
           }
@@ -445,13 +454,13 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
       fv[2] += (fpz + cz) * dz;
       flj += sw * elj;
       fcl += sw * ecl;
-      // partial sums close every 4 pairs within rcut (not every 4 list entries),
+      // partial sums close every 8 pairs within rcut (not every 8 list entries),
       // so the force is a function of the positions alone, whatever the list holds
-      if ((np & 3) == 0) { flush(); zero(); }
+      if ((np & 7) == 0) { flush(); zero(); }
     }
   }
   flush();
-  a.npair += np;
+  npair += np;
 }
 
 // FP64 pair loop: the reference's generic Switching (src/force_calculator.cxx:691-779)
@@ -538,10 +547,13 @@ template <int S, int C0, int PREC>
 __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                            bool rebuild, int tile_size) {
   __shared__ double red[8 * 8];
+  __shared__ F32Const k32;
+  extern __shared__ double acc[];   // FP32 form: (3S + 8) x blockDim.x FP64 accumulators
   const int i = threadIdx.x;
   const bool valid = i < t.count;
   const int li = t.start + i;
   const int g = c.mol_off + li;
+  const int T = blockDim.x;
   uint16_t* nb = d.nbr + c.nbr_off + (long long)(blockIdx.x - c.tile_off) * c.nbr_cap * tile_size + i;
   if (rebuild) {
     build_lists<PREC>(d, c, t, L, nb, tile_size);
@@ -561,6 +573,19 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
     if (i == 0)
       for (int x = 0; x < 3; x++) d.Lbuild[3 * blockIdx.x + x] = L[x];
   }
+  if (PREC == kF32) {
+    if (i == 0) {
+      for (int k = 0; k < kMaxSites; k++)
+        for (int l = 0; l < kMaxSites; l++) k32.qq[k][l] = (float)c.qq[k][l];
+      for (int x = 0; x < 3; x++) {
+        k32.Ls[x] = (float)(L[x] * kFixInv);
+        k32.Lf[x] = (float)L[x];
+        k32.hL[x] = 0.5f * (float)L[x];
+      }
+    }
+    for (int f = 0; f < 3 * S + 8; f++) acc[f * T + i] = 0.0;
+    __syncthreads();
+  }
   IAcc a;
 #pragma unroll
   for (int k = 0; k < kMaxSites; k++) a.fs[k][0] = a.fs[k][1] = a.fs[k][2] = 0.0;
@@ -574,8 +599,17 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
     const double reach = c.rc + 2.0 * c.site_reach;
     const bool simg = (L[0] < 2.0 * reach) || (L[1] < 2.0 * reach) || (L[2] < 2.0 * reach);
     if (PREC == kF32) {
-      if (simg) pair_loop_f32<S, C0, true>(d, c, t, L, nb, cnt, a);
-      else pair_loop_f32<S, C0, false>(d, c, t, L, nb, cnt, a);
+      if (simg) pair_loop_f32<S, C0, true>(d, c, t, k32, nb, cnt, acc, a.npair);
+      else pair_loop_f32<S, C0, false>(d, c, t, k32, nb, cnt, acc, a.npair);
+#pragma unroll
+      for (int k = 0; k < S; k++)
+        for (int x = 0; x < 3; x++) a.fs[k][x] = acc[(3 * k + x) * T + i];
+      for (int x = 0; x < 3; x++) {
+        a.fc[x] = acc[(3 * S + x) * T + i];
+        a.vir[x] = acc[(3 * S + 3 + x) * T + i];
+      }
+      a.lj = acc[(3 * S + 6) * T + i];
+      a.clmb = acc[(3 * S + 7) * T + i];
     } else {
       if (simg) pair_loop_f64<S, C0, true>(d, c, t, L, nb, cnt, a);
       else pair_loop_f64<S, C0, false>(d, c, t, L, nb, cnt, a);
@@ -1181,11 +1215,14 @@ void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, boo
   else
     k_integrate<false><<<d.ntiles, tile, 0, s>>>(d, X, Y, prec);
 }
+size_t force_smem_bytes(int tile) { return (size_t)(3 * kMaxSites + 8) * tile * sizeof(double); }
+
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s) {
   if (prec == kF32) {
-    if (force_only) k_force<kF32, true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
-    else k_force<kF32, false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    const size_t sm = force_smem_bytes(tile);
+    if (force_only) k_force<kF32, true><<<d.ntiles, tile, sm, s>>>(d, Yin, Xout, tile);
+    else k_force<kF32, false><<<d.ntiles, tile, sm, s>>>(d, Yin, Xout, tile);
   } else {
     if (force_only) k_force<kF64, true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
     else k_force<kF64, false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);

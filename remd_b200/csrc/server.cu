@@ -32,6 +32,7 @@ remd_status engine_set_h0(remd_handle h, const double* H0);
 remd_status engine_set_exchange(remd_handle h, const int* grids, const unsigned long long* seeds,
                                 const long long* steps, const int* index);
 remd_status engine_get_exchange(remd_handle h, long long* steps, int* index);
+remd_status engine_set_pending_conditions(remd_handle h, const double* T, const double* P);
 size_t engine_bytes(remd_handle h);
 }  // namespace remd
 
@@ -42,6 +43,7 @@ namespace {
 struct Rep {
   std::vector<double> r, v, q, p, m, I;
   double s, Ps, Q, Pv[3], W, L[3], T, P, H0;
+  double Tnext, Pnext;             // condition chosen by the last exchange, applied next interval
   bool has_h0 = false;
 };
 
@@ -134,16 +136,19 @@ static remd_status pull_batch(remd_server_s* S) {
       if ((st = remd_get_state(S->batch, rep, &sv)) != REMD_OK) return st;
       R.s = sv.s; R.Ps = sv.Ps;
       for (int x = 0; x < 3; x++) { R.Pv[x] = sv.Pv[x]; R.L[x] = sv.L[x]; }
+      R.T = sv.T;
+      R.P = sv.P;
       R.H0 = sv.H0;
       R.has_h0 = true;
     }
   }
-  // the device conditions (after the last exchange) become the replicas' T, P
+  // the conditions the last exchange chose; applied (with the exchange tail) at
+  // the start of the replica's next interval
   std::vector<double> T(total), P(total);
   if ((st = remd_get_conditions(S->batch, nullptr, T.data(), P.data())) != REMD_OK) return st;
   rep = 0;
   for (Job* j : S->active)
-    for (int k = 0; k < j->nrep(); k++, rep++) { j->reps[k].T = T[rep]; j->reps[k].P = P[rep]; }
+    for (int k = 0; k < j->nrep(); k++, rep++) { j->reps[k].Tnext = T[rep]; j->reps[k].Pnext = P[rep]; }
   return REMD_OK;
 }
 
@@ -156,7 +161,7 @@ static remd_status build_batch(remd_server_s* S) {
   std::vector<int> grids, index;
   std::vector<unsigned long long> seeds;
   std::vector<long long> steps;
-  std::vector<double> H0;
+  std::vector<double> H0, Tnext, Pnext;
   bool any_h0 = false;
   for (Job* j : S->active) {
     sys.push_back(j->sys);
@@ -175,6 +180,8 @@ static remd_status build_batch(remd_server_s* S) {
       init.push_back(ri);
       index.push_back(j->index[k]);
       H0.push_back(R.H0);
+      Tnext.push_back(R.Tnext);
+      Pnext.push_back(R.Pnext);
       any_h0 = any_h0 || R.has_h0;
     }
   }
@@ -193,6 +200,7 @@ static remd_status build_batch(remd_server_s* S) {
       }
     if ((st = engine_set_h0(S->batch, fresh.data())) != REMD_OK) return st;
   }
+  if ((st = engine_set_pending_conditions(S->batch, Tnext.data(), Pnext.data())) != REMD_OK) return st;
   return engine_set_exchange(S->batch, grids.data(), seeds.data(), steps.data(), index.data());
 }
 
@@ -250,6 +258,8 @@ remd_status remd_job_submit(remd_server S, const remd_job_desc* jd, remd_job_id*
     R.q.assign(ri.q, ri.q + 4 * n); R.p.assign(ri.p, ri.p + 4 * n);
     R.m.assign(ri.mass, ri.mass + n); R.I.assign(ri.inertia, ri.inertia + 3 * n);
     R.s = ri.s; R.Ps = ri.Ps; R.Q = ri.Q; R.W = ri.W; R.T = ri.T; R.P = ri.P; R.H0 = 0.0;
+    R.Tnext = ri.T;
+    R.Pnext = ri.P;
     for (int x = 0; x < 3; x++) { R.Pv[x] = ri.Pv[x]; R.L[x] = ri.L[x]; }
     j->reps.push_back(R);
     j->index.push_back(k);
