@@ -53,22 +53,30 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--config", type=int, default=4, choices=[1, 2, 3, 4])
+    ap.add_argument("--config", type=int, default=4, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--jobs", type=int, default=8, help="config 5: jobs of the serving stream")
+    ap.add_argument("--budget-gib", type=float, default=24.0, help="config 5: server HBM budget")
     ap.add_argument("--interval", type=int, default=100)
     ap.add_argument("--tile", type=int, default=128)
     ap.add_argument("--skin", type=float, default=1.0)
-    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=None, help="workload seed (default: the config index)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
     ap.add_argument("--equil-rounds", type=int, default=10,
                     help="untimed relaxation rounds of 20 steps + init_scaling")
-    return ap.parse_args(argv)
+    a = ap.parse_args(argv)
+    if a.seed is None:
+        a.seed = a.config
+    return a
 
 
 def workload(config, seed, interval):
     from remd_b200 import systems as S
+    if config == 5:
+        return [S.config5_job(seed, k, interval=interval)[0] for k in range(8)]
     if config == 4:
         return S.config4(seed=seed, interval=interval)
     fn = {1: S.config1, 2: S.config2, 3: S.config3}[config]
@@ -87,7 +95,8 @@ def workload_desc(config, ens, interval):
     n = [e.spec.nmol for e in ens for _ in e.states]
     name = {4: "uneven batch: 8 ensembles / 256 replicas, TIP3P/4P/5P, bulk+tube+slit",
             1: "TIP4P nanotube N=128, 16 replicas", 2: "TIP4P slit N=512, 64 replicas",
-            3: "TIP5P bulk N=1728, 128 replicas"}[config]
+            3: "TIP5P bulk N=1728, 128 replicas",
+            5: "serving stream: the first 8 jobs' replicas"}[config]
     return {"workload": name, "config_index": config, "replicas": len(n),
             "molecules": int(sum(n)), "nmol_range": [int(min(n)), int(max(n))],
             "interval_steps": interval, "ensembles": len(ens),
@@ -262,6 +271,109 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ serving (config 5)
+def _gen_job(a):
+    from remd_b200 import systems as S
+    return S.config5_job(*a)
+
+
+def make_jobs(seed, njobs):
+    """The seeded job stream, generated on the host cores (spawned workers, so
+    this is safe before or after CUDA is initialised)."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(max(1, min(njobs, cpu_threads()))) as pool:
+        return pool.map(_gen_job, [(seed, k) for k in range(njobs)])
+
+
+def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
+    """Feed the jobs to a server at their arrival times (host clock) and step it
+    until all are done.  one_at_a_time: a job is submitted only when the server
+    is empty (the plain one-job-at-a-time form).  Returns per-job latencies
+    (arrival -> done, s), the makespan and the server's statistics."""
+    from remd_b200 import engine as E
+    srv = E.Server(budget_bytes=budget, device=dev)
+    n = len(jobs)
+    ids, done_t, state = [None] * n, [None] * n, [0] * n
+    active = set()
+    nxt = 0
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now and not (one_at_a_time and active):
+            ens, nint = jobs[nxt]
+            ids[nxt] = srv.submit(ens, nint, seed=seed0 + nxt)
+            active.add(nxt)
+            nxt += 1
+        if not active:
+            if nxt >= n:
+                break
+            time.sleep(max(arrivals[nxt] - now, 0.0))
+            continue
+        srv.step()
+        now = time.perf_counter() - t0
+        for k in sorted(active):
+            st = srv.poll(ids[k]).state
+            if st >= 2:
+                done_t[k], state[k] = now, st
+                active.discard(k)
+    stats = srv.stats()
+    srv.close()
+    lat = [done_t[k] - arrivals[k] for k in range(n)]
+    ok = [k for k in range(n) if state[k] == 2]
+    units = sum(jobs[k][0].spec.nmol * jobs[k][0].nreplica * jobs[k][0].spec.interval * jobs[k][1]
+                for k in ok)
+    span = max(done_t) - arrivals[0]
+    return {"value": units / span, "makespan_s": span, "jobs_done": len(ok), "mol_steps": units,
+            "p50_job_s": float(np.percentile(lat, 50)), "p99_job_s": float(np.percentile(lat, 99)),
+            "p50_interval_ms": stats["p50_interval_ms"], "p99_interval_ms": stats["p99_interval_ms"],
+            "intervals": stats["intervals_done"], "busy_s": stats["busy_s"]}
+
+
+def serving_arm(args, rank, world, local):
+    import torch
+    from remd_b200 import systems as S
+    dev = local
+    njobs = args.jobs
+    jobs = make_jobs(args.seed + 1000 * rank, njobs)
+    arrivals = S.config5_arrivals(args.seed + 1000 * rank, njobs)
+    torch.cuda.set_device(dev)
+    budget = int(args.budget_gib * (1 << 30))
+    # warm-up: the first W jobs, one interval each (library load, context, graph capture)
+    warm = [(e, 1) for e, _ in jobs[:max(args.warmup, 1)]]
+    run_stream(warm, np.zeros(len(warm)), budget, dev, False, seed0=77)
+    clocks = ClockSampler(dev)
+    barrier(world)
+    batched = run_stream(jobs, arrivals, budget, dev, False)
+    barrier(world)
+    clk = clocks.stop()
+    single = run_stream(jobs, arrivals, budget, dev, True)
+    value, max_s, total = aggregate(batched["makespan_s"] * 1e3, batched["mol_steps"], world)
+    if rank == 0:
+        n = [e.spec.nmol for e, _ in jobs]
+        desc = {"workload": f"serving: Poisson stream, {S.SERVING_RATE:g} jobs/s, first {njobs} jobs; "
+                            "nmol logU 96-4096, TIP3P/4P/5P, bulk+tube+slit, 8-64 replicas, "
+                            "interval 100, ninterval 10-200",
+                "config_index": 5, "jobs": njobs, "nmol_range": [min(n), max(n)],
+                "replicas": int(sum(e.nreplica for e, _ in jobs)),
+                "ninterval": [int(k) for _, k in jobs],
+                "budget_gib": args.budget_gib, "parallelism": "replicas-only",
+                "l2": "not flushed: a serving interval reads each job's state once per step "
+                      "from its own buffers (working set of the batch > L2 for the larger jobs)"}
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+                "steps": njobs, "warmup": len(warm), "ms_per_step": max_s / njobs,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": desc,
+                "latency": {k: batched[k] for k in ("p50_job_s", "p99_job_s", "p50_interval_ms",
+                                                   "p99_interval_ms")},
+                "served": batched, "one_at_a_time": single,
+                "speedup_vs_one_at_a_time": batched["value"] / single["value"],
+                "e2e": {"value": value, "unit": METRIC,
+                        "note": "the server API is the host-facing call: job states are copied in "
+                                "at admission and averages out every interval"},
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ engine arm
 def profile_traffic():
     """DRAM bytes per force launch from the committed ncu summary, if present."""
@@ -275,6 +387,44 @@ def profile_traffic():
             except ValueError:
                 return None
     return None
+
+
+def force_accuracy(eng, ens, dev):
+    """FP32 forces of the bench's own (equilibrated, advanced) configurations
+    against the FP64 form of the engine on the same snapshots (the FP64 form is
+    pinned to the FP64 oracle by the parity tests).  Per replica: force and
+    torque RMS relative error (||F32 - F64||_2 / ||F64||_2 over all molecules),
+    potential-energy and virial relative error; reported as the max over
+    replicas."""
+    from remd_b200 import engine as E
+    from remd_b200.inputs import ReplicaState
+    eng.compute_forces()
+    sts, got = [], []
+    k = 0
+    for e in ens:
+        for st0 in e.states:
+            g = eng.ConvertVariablesToHost(k)
+            sts.append(ReplicaState(g["r"], g["v"], g["q"], g["p"], st0.m, st0.I, g["s"], g["Ps"],
+                                    g["Q"], g["Pv"], g["W"], g["L"], g["T"], g["P"]))
+            got.append(g)
+            k += 1
+    ref = E.REMDGPU(ens, precision="fp64", device=dev, states=sts)
+    ref.compute_forces()
+    fe, ne, ue, ve = [], [], [], []
+    for k, g in enumerate(got):
+        h = ref.ConvertVariablesToHost(k)
+        fe.append(np.linalg.norm(g["f"] - h["f"]) / np.linalg.norm(h["f"]))
+        ne.append(np.linalg.norm(g["n"] - h["n"]) / np.linalg.norm(h["n"]))
+        ue.append(abs(g["pot"] - h["pot"]) / abs(h["pot"]))
+        ve.append(np.linalg.norm(g["vir"] - h["vir"]) / np.linalg.norm(h["vir"]))
+    ref.close()
+    return {"reference": "FP64 form of this engine on the same snapshots",
+            "replicas": len(got),
+            "force_rms_rel_max": float(max(fe)), "force_rms_rel_median": float(np.median(fe)),
+            "torque_rms_rel_max": float(max(ne)),
+            "pot_rel_max": float(max(ue)), "pot_rel_median": float(np.median(ue)),
+            "virial_rel_max": float(max(ve)),
+            "gates": {"force_rms_rel": 1e-5, "pot_rel": 1e-6}}
 
 
 def engine_arm(args, rank, world, local):
@@ -351,6 +501,8 @@ def engine_arm(args, rank, world, local):
             "traffic": profile_traffic(), "pairs_per_launch": pairs,
             "flops_per_launch": flops, "force_ms": force_ms, "integrate_ms": integ_ms}
 
+    acc = None if args.no_accuracy else force_accuracy(eng, ens, dev)
+
     # end to end through the public C-ABI call (host buffers, host exchange)
     e2e = None
     eng.enable_device_exchange(None)
@@ -416,6 +568,10 @@ def engine_arm(args, rank, world, local):
                 "config": workload_desc(args.config, ens, args.interval),
                 "gpu_launches": eng.launches_per_interval() * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "latency": {"p50_interval_ms": float(np.percentile(ms, 50)),
+                            "p99_interval_ms": float(np.percentile(ms, 99)),
+                            "samples": len(ms)},
+                "accuracy": acc,
                 "plain_fp64": plain,
                 "speedup_vs_plain_fp64": (value / world / plain["value"]) if plain else None,
                 "wall_s": wall, "interval_ms": [round(x, 3) for x in ms],
@@ -430,6 +586,8 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
+        elif args.config == 5:
+            serving_arm(args, rank, world, local)
         else:
             engine_arm(args, rank, world, local)
     finally:

@@ -254,7 +254,7 @@ remd_status remd_write_chk(remd_handle h, int rep, const char *path);
  * {LJ, Coulomb, wall, virial x3, unordered pairs within rcut, error word (0 ok,
  * 1 neighbour overflow)}; L is the host box.  Same FP32 arithmetic as a
  * REMD_PREC_FP32 handle's remd_compute_forces.  All working memory is one
- * fixed device array of the library (about 5.6 MB, held by every GPU that
+ * fixed device array of the library (about 8.8 MB, held by every GPU that
  * loads it until exit): at most 2048 molecules and 1024 neighbours per molecule
  * (rcut <= ~12.4 A); larger inputs are rejected with REMD_ERR_INVALID.  The
  * first call on a device looks up that array's device address (set-up), so make

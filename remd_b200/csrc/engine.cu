@@ -36,6 +36,7 @@ struct remd_engine_s {
   std::vector<int> rep_ens, ens_rep_off, ens_nrep;
   std::vector<RepConst> rc;
   std::vector<Tile> tiles;
+  std::vector<int> order;          // force blocks -> tiles, costliest first
   std::vector<double> curT, curP;
   std::vector<double> wall_h;
   DevPtrs d{};
@@ -122,6 +123,21 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
     c.nbr_off = nbr_words;
     nbr_words += (long long)c.ntile * c.nbr_cap * T;
   }
+  // force blocks in decreasing order of estimated pair work (longest first, so
+  // the costliest tiles do not form the tail of the launch): molecules x
+  // neighbours within rcut at liquid density x FLOPs per molecule pair
+  {
+    std::vector<double> cost(h->tiles.size());
+    for (size_t t = 0; t < h->tiles.size(); t++) {
+      const RepConst& c = h->rc[h->tiles[t].rep];
+      const double nbr = std::min((double)(c.nmol - 1), 0.0334 * 4.0 / 3.0 * M_PI * c.rc * c.rc * c.rc);
+      const int nq = c.nsite - c.c0;
+      cost[t] = h->tiles[t].count * nbr * (51.0 + 32.0 + 27.0 * nq * nq);
+    }
+    h->order.resize(h->tiles.size());
+    for (size_t t = 0; t < h->order.size(); t++) h->order[t] = (int)t;
+    std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  }
   const size_t N = h->N, nt = h->tiles.size(), nr = h->nrep;
   const size_t elem = (h->prec == kF32) ? 4 : 8;
   const size_t sizes[] = {
@@ -144,6 +160,8 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       (size_t)std::max(nr / 2, (size_t)1) * 8,   // 27 u
       (size_t)h->nens * 8,             // 28 per-ensemble exchange step counter
       (size_t)h->nens * 8,             // 29 per-ensemble exchange seed
+      (h->prec == kF32) ? (size_t)nbr_words * 2 : 0,   // 30 nbt (FP32 per-step lists)
+      nt * 4,                          // 31 order
   };
   offs.clear();
   total = 0;
@@ -203,10 +221,13 @@ static remd_status allocate(remd_engine_s* h) {
   h->d_u = reinterpret_cast<double*>(b + offs[27]);
   h->d_step = reinterpret_cast<long long*>(b + offs[28]);
   h->d_seed = reinterpret_cast<unsigned long long*>(b + offs[29]);
+  d.nbt = reinterpret_cast<uint16_t*>(b + offs[30]);
+  d.order = reinterpret_cast<int*>(b + offs[31]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync((void*)d.tiles, h->tiles.data(), h->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync((void*)d.order, h->order.data(), h->order.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   if (!h->wall_h.empty())
     CK(cudaMemcpyAsync((void*)d.wall, h->wall_h.data(), h->wall_h.size() * 8, cudaMemcpyHostToDevice, h->stream));
   // later set-up copies use the default stream, which does not order with this
@@ -474,7 +495,8 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   }
   h->nrep = rep;
   h->N = mol;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      force_kernel_setup() != cudaSuccess) {
     set_error("cannot set up device/stream");
     delete h;
     return REMD_ERR_CUDA;

@@ -84,11 +84,13 @@ struct DevPtrs {
   int ntiles, nrep;
   const RepConst* rc;
   const Tile* tiles;
+  const int* order;              // force-launch block -> tile, costliest first (NULL: identity)
   double *r, *v, *q, *p, *f, *n; // SoA, component-major, stride N
   void* pack;                    // FP32 words or FP64 doubles
   int4* ref_com;                 // fixed-point com at the last list build
   double* Lbuild;                // per tile, 3 doubles (NaN = list invalid)
-  uint16_t* nbr;                 // neighbour lists
+  uint16_t* nbr;                 // neighbour lists (rcut + skin)
+  uint16_t* nbt;                 // FP32 form: per-step lists of the pairs within rcut (same layout)
   int* nbr_cnt;                  // per molecule
   const double* wall;            // {f, U} pairs
   Part1* part1;

@@ -304,13 +304,19 @@ struct IAcc {
   long long npair;
 };
 
-// FP32 pair loop over i's neighbour list.  Pair math in FP32 (rsqrt on the SFU
-// plus one Newton step), partial sums in FP32 over 8 pairs within rcut, then
-// FP64 accumulation into this thread's slots of `acc` (shared memory, field f
-// at acc[f * blockDim.x + threadIdx.x]: 3S site-force components, 3 switching-
-// correction, 3 virial, LJ, Coulomb).  Lists are in ascending j, so the result
-// depends only on the positions (not on when the list was built).  The record
-// of neighbour k+1 is loaded while neighbour k is computed.
+// FP32 pair loop over i's neighbour list, in two passes.
+// Pass 1 scans the (rcut + skin) list and writes the neighbours within rcut, in
+// the list's ascending-j order, to i's column of the per-step list `nbt`
+// (same layout and capacity as the skin list; it cannot overflow).  Pass 2
+// computes exactly those pairs, so the lanes of a warp stay converged (no
+// cutoff branch) and differ only in their pair counts.
+// Pair math in FP32 (rsqrt on the SFU plus one Newton step); partial sums in
+// FP32 over 8 pairs, then FP64 accumulation into this thread's slots of `acc`
+// (shared memory, field f at acc[f * blockDim.x + threadIdx.x]: 3S site-force
+// components, 3 switching-correction, 3 virial, LJ, Coulomb).  The pairs within
+// rcut, in ascending j, and their grouping by 8 depend only on the positions,
+// not on when the skin list was built.  Neighbour indices are read two pairs
+// ahead and records one pair ahead of their use.
 // SIMG: apply the minimum image to every site pair as the reference does
 // (src/force_calculator.cxx:737-741).  It changes the result only when a box
 // length is below 2 (rc + 2 site_reach); the caller enables it just then.
@@ -321,12 +327,14 @@ struct F32Const {
 
 template <int S, int C0, bool SIMG>
 __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const F32Const& k32,
-                              const uint16_t* nb, int cnt, double* acc, long long& npair) {
+                              const uint16_t* nb, uint16_t* nt, int cnt, double* acc, long long& npair) {
   constexpr int STRIDE = ((3 + 3 * S) + 3) / 4 * 4;
   constexpr int NV = STRIDE / 4;
   const int T = blockDim.x, tid = threadIdx.x;
   const int li = t.start + tid;
   const uint4* base = reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off);
+  const float Ls0 = k32.Ls[0], Ls1 = k32.Ls[1], Ls2 = k32.Ls[2];
+  const float rc2 = (float)(c.rc * c.rc);
   int xi, yi, zi;
   float si[S][3];
   {
@@ -342,9 +350,47 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 #pragma unroll
       for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
   }
-  const float rc = (float)c.rc, rs = (float)c.rs, rc2 = (float)(c.rc * c.rc);
+  // pass 1: neighbours within rcut (same FP32 distance as pass 2), eight
+  // candidates per round so that their loads are in flight together
+  int np = 0;
+  {
+    constexpr int B = 8;
+    int k = 0;
+    for (; k + B <= cnt; k += B) {
+      int j[B];
+      uint4 u[B];
+#pragma unroll
+      for (int m = 0; m < B; m++) j[m] = nb[(long long)(k + m) * T];
+#pragma unroll
+      for (int m = 0; m < B; m++) u[m] = __ldg(base + (long long)j[m] * NV);
+#pragma unroll
+      for (int m = 0; m < B; m++) {
+        const float dx = (float)(int)(xi - (int)u[m].x) * Ls0;
+        const float dy = (float)(int)(yi - (int)u[m].y) * Ls1;
+        const float dz = (float)(int)(zi - (int)u[m].z) * Ls2;
+        if (dx * dx + dy * dy + dz * dz <= rc2) {
+          nt[(long long)np * T] = (uint16_t)j[m];
+          np++;
+        }
+      }
+    }
+    for (; k < cnt; k++) {
+      const int j = nb[(long long)k * T];
+      const uint4 u = __ldg(base + (long long)j * NV);
+      const float dx = (float)(int)(xi - (int)u.x) * Ls0;
+      const float dy = (float)(int)(yi - (int)u.y) * Ls1;
+      const float dz = (float)(int)(zi - (int)u.z) * Ls2;
+      if (dx * dx + dy * dy + dz * dz <= rc2) {
+        nt[(long long)np * T] = (uint16_t)j;
+        np++;
+      }
+    }
+  }
+  const float rc = (float)c.rc, rs = (float)c.rs;
   const float coef = (float)c.coef_sw;
   const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
+  const float hL0 = k32.hL[0], hL1 = k32.hL[1], hL2 = k32.hL[2];
+  const float Lf0 = k32.Lf[0], Lf1 = k32.Lf[1], Lf2 = k32.Lf[2];
 
   float fs[S][3], fc[3], fv[3], flj, fcl;
   auto zero = [&]() {
@@ -368,103 +414,98 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
     acc[(3 * S + 7) * T + tid] += (double)fcl;
   };
   zero();
-  long long np = 0;
+  // pass 2: the pairs within rcut
   uint4 nx[NV];
-  if (cnt > 0) {
-    const int j0 = nb[0];
+  int jnext = (np > 1) ? nt[T] : 0;
+  if (np > 0) {
+    const int j0 = nt[0];
 #pragma unroll
     for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)j0 * NV + m);
   }
-  for (int k = 0; k < cnt; k++) {
+  for (int k = 0; k < np; k++) {
     uint32_t wj[STRIDE];
 #pragma unroll
     for (int m = 0; m < NV; m++) {
       wj[4 * m] = nx[m].x; wj[4 * m + 1] = nx[m].y; wj[4 * m + 2] = nx[m].z; wj[4 * m + 3] = nx[m].w;
     }
-    if (k + 1 < cnt) {
-      const int jn = nb[(long long)(k + 1) * T];
+    if (k + 1 < np) {
+      const int jn = jnext;
+      if (k + 2 < np) jnext = nt[(long long)(k + 2) * T];
 #pragma unroll
       for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
     }
-    const float dx = (float)(int)(xi - (int)wj[0]) * k32.Ls[0];
-    const float dy = (float)(int)(yi - (int)wj[1]) * k32.Ls[1];
-    const float dz = (float)(int)(zi - (int)wj[2]) * k32.Ls[2];
+    const float dx = (float)(int)(xi - (int)wj[0]) * Ls0;
+    const float dy = (float)(int)(yi - (int)wj[1]) * Ls1;
+    const float dz = (float)(int)(zi - (int)wj[2]) * Ls2;
     const float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 <= rc2) {
-      np++;
-      const float rinv = rsqrtf(r2);
-      const float r = r2 * rinv;
-      float sw = 1.f, dsw = 0.f;
-      if (r > rs) {
-        const float r01c = r - rc, r01l = r - rs;
-        sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
-        dsw = coef * 30.f * r01c * r01c * r01l * r01l;
-      }
-      float elj = 0.f, ecl = 0.f;
-      float fpx = 0.f, fpy = 0.f, fpz = 0.f;
-#pragma unroll
-      for (int kk = 0; kk < S; kk++) {
-        if (kk != 0 && kk < C0) continue;
-        const float ax = dx + si[kk][0], ay = dy + si[kk][1], az = dz + si[kk][2];
-        float tx = 0.f, ty = 0.f, tz = 0.f;
-#pragma unroll
-        for (int l = 0; l < S; l++) {
-          const bool lj_pair = (kk == 0 && l == 0);
-          const bool cl_pair = (kk >= C0 && l >= C0);
-          if (!lj_pair && !cl_pair) continue;
-          float x = ax - __uint_as_float(wj[3 + 3 * l]);
-          float y = ay - __uint_as_float(wj[3 + 3 * l + 1]);
-          float z = az - __uint_as_float(wj[3 + 3 * l + 2]);
-          if (SIMG) {
-            if (x >= k32.hL[0]) x -= k32.Lf[0];
-            if (x < -k32.hL[0]) x += k32.Lf[0];
-            if (y >= k32.hL[1]) y -= k32.Lf[1];
-            if (y < -k32.hL[1]) y += k32.Lf[1];
-            if (z >= k32.hL[2]) z -= k32.Lf[2];
-            if (z < -k32.hL[2]) z += k32.Lf[2];
-          }
-          const float rr = x * x + y * y + z * z;
-          float ri = rsqrtf(rr);
-          ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);   // one Newton step: ~0.5 ulp
-          const float ri2 = ri * ri;
-          float ftmp = 0.f;
-          if (lj_pair) {
-            float s6 = sgm2 * ri2;
-            s6 = s6 * s6 * s6;
-            elj += eps4 * s6 * (s6 - 1.f);
-            ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
-          }
-          if (cl_pair) {
-            const float e = k32.qq[kk][l] * ri;
-            ecl += e;
-            ftmp += e * ri2;
-          }
-          ftmp *= sw;
-          tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
-        }
-        fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
-        fpx += tx; fpy += ty; fpz += tz;
-      }
-      const float e = elj + ecl;
-      const float g = dsw * rinv * e;
-      const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
-      fc[0] += cx; fc[1] += cy; fc[2] += cz;
-      fv[0] += (fpx + cx) * dx;
-      fv[1] += (fpy + cy) * dy;
-      fv[2] += (fpz + cz) * dz;
-      flj += sw * elj;
-      fcl += sw * ecl;
-      // partial sums close every 8 pairs within rcut (not every 8 list entries),
-      // so the force is a function of the positions alone, whatever the list holds
-      if ((np & 7) == 0) { flush(); zero(); }
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    float sw = 1.f, dsw = 0.f;
+    if (r > rs) {
+      const float r01c = r - rc, r01l = r - rs;
+      sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
+      dsw = coef * 30.f * r01c * r01c * r01l * r01l;
     }
+    float elj = 0.f, ecl = 0.f;
+    float fpx = 0.f, fpy = 0.f, fpz = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < S; kk++) {
+      if (kk != 0 && kk < C0) continue;
+      const float ax = dx + si[kk][0], ay = dy + si[kk][1], az = dz + si[kk][2];
+      float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+      for (int l = 0; l < S; l++) {
+        const bool lj_pair = (kk == 0 && l == 0);
+        const bool cl_pair = (kk >= C0 && l >= C0);
+        if (!lj_pair && !cl_pair) continue;
+        float x = ax - __uint_as_float(wj[3 + 3 * l]);
+        float y = ay - __uint_as_float(wj[3 + 3 * l + 1]);
+        float z = az - __uint_as_float(wj[3 + 3 * l + 2]);
+        if (SIMG) {
+          if (x >= hL0) x -= Lf0;
+          if (x < -hL0) x += Lf0;
+          if (y >= hL1) y -= Lf1;
+          if (y < -hL1) y += Lf1;
+          if (z >= hL2) z -= Lf2;
+          if (z < -hL2) z += Lf2;
+        }
+        const float rr = x * x + y * y + z * z;
+        float ri = rsqrtf(rr);
+        ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);   // one Newton step: ~0.5 ulp
+        const float ri2 = ri * ri;
+        float ftmp = 0.f;
+        if (lj_pair) {
+          float s6 = sgm2 * ri2;
+          s6 = s6 * s6 * s6;
+          elj += eps4 * s6 * (s6 - 1.f);
+          ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
+        }
+        if (cl_pair) {
+          const float e = k32.qq[kk][l] * ri;
+          ecl += e;
+          ftmp += e * ri2;
+        }
+        ftmp *= sw;
+        tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
+      }
+      fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
+      fpx += tx; fpy += ty; fpz += tz;
+    }
+    const float e = elj + ecl;
+    const float g = dsw * rinv * e;
+    const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
+    fc[0] += cx; fc[1] += cy; fc[2] += cz;
+    fv[0] += (fpx + cx) * dx;
+    fv[1] += (fpy + cy) * dy;
+    fv[2] += (fpz + cz) * dz;
+    flj += sw * elj;
+    fcl += sw * ecl;
+    if ((k & 15) == 15) { flush(); zero(); }
   }
   flush();
   npair += np;
 }
 
-// FP64 pair loop: the reference's generic Switching (src/force_calculator.cxx:691-779)
-// arithmetic for molecule i, over its neighbour list.
 template <int S, int C0, bool SIMG>
 __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                               const uint16_t* nb, int cnt, IAcc& a) {
@@ -544,7 +585,7 @@ __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t
 }
 
 template <int S, int C0, int PREC>
-__device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+__device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
                            bool rebuild, int tile_size) {
   __shared__ double red[8 * 8];
   __shared__ F32Const k32;
@@ -554,7 +595,7 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
   const int li = t.start + i;
   const int g = c.mol_off + li;
   const int T = blockDim.x;
-  uint16_t* nb = d.nbr + c.nbr_off + (long long)(blockIdx.x - c.tile_off) * c.nbr_cap * tile_size + i;
+  uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
   if (rebuild) {
     build_lists<PREC>(d, c, t, L, nb, tile_size);
     __syncthreads();
@@ -571,7 +612,7 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
       d.ref_com[g] = rc4;
     }
     if (i == 0)
-      for (int x = 0; x < 3; x++) d.Lbuild[3 * blockIdx.x + x] = L[x];
+      for (int x = 0; x < 3; x++) d.Lbuild[3 * tix + x] = L[x];
   }
   if (PREC == kF32) {
     if (i == 0) {
@@ -599,8 +640,9 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
     const double reach = c.rc + 2.0 * c.site_reach;
     const bool simg = (L[0] < 2.0 * reach) || (L[1] < 2.0 * reach) || (L[2] < 2.0 * reach);
     if (PREC == kF32) {
-      if (simg) pair_loop_f32<S, C0, true>(d, c, t, k32, nb, cnt, acc, a.npair);
-      else pair_loop_f32<S, C0, false>(d, c, t, k32, nb, cnt, acc, a.npair);
+      uint16_t* nt = d.nbt + (nb - d.nbr);
+      if (simg) pair_loop_f32<S, C0, true>(d, c, t, k32, nb, nt, cnt, acc, a.npair);
+      else pair_loop_f32<S, C0, false>(d, c, t, k32, nb, nt, cnt, acc, a.npair);
 #pragma unroll
       for (int k = 0; k < S; k++)
         for (int x = 0; x < 3; x++) a.fs[k][x] = acc[(3 * k + x) * T + i];
@@ -673,7 +715,7 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, c
     p.vir[0] = s6[3]; p.vir[1] = s6[4]; p.vir[2] = s6[5];
     p.npairs = (long long)llrint(s6[6]);
     p.pad = 0.0;
-    d.part2[blockIdx.x] = p;
+    d.part2[tix] = p;
   }
 }
 
@@ -681,7 +723,8 @@ template <int PREC, bool FORCE_ONLY>
 __global__ void __launch_bounds__(256) k_force(DevPtrs d, const RepState* __restrict__ Yin,
                                                RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
-  const Tile t = d.tiles[blockIdx.x];
+  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;   // costliest tiles first
+  const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
   if (threadIdx.x == 0) {
     RepState st = Yin[t.rep];
@@ -695,11 +738,10 @@ __global__ void __launch_bounds__(256) k_force(DevPtrs d, const RepState* __rest
       }
       pspv(c, st, sPv, sPs);
       d4(c, st);
-      if (blockIdx.x == c.tile_off) Xout[t.rep] = st;
+      if (tix == c.tile_off) Xout[t.rep] = st;
       // list validity: pairs now within rc were within rc+skin at the build if
       // 2*max|displacement| + rc*(max_d Lbuild_d/L_d - 1) <= skin
-      const double lb0 = d.Lbuild[3 * blockIdx.x], lb1 = d.Lbuild[3 * blockIdx.x + 1],
-                   lb2 = d.Lbuild[3 * blockIdx.x + 2];
+      const double lb0 = d.Lbuild[3 * tix], lb1 = d.Lbuild[3 * tix + 1], lb2 = d.Lbuild[3 * tix + 2];
       int rb = !(lb0 == lb0);
       if (!rb) {
         const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
@@ -715,11 +757,11 @@ __global__ void __launch_bounds__(256) k_force(DevPtrs d, const RepState* __rest
   const double L[3] = {h.L[0], h.L[1], h.L[2]};
   const bool rb = h.rebuild != 0;
   if (c.nsite == 3)
-    force_tile<3, 0, PREC>(d, c, t, L, rb, tile_size);
+    force_tile<3, 0, PREC>(d, c, t, tix, L, rb, tile_size);
   else if (c.nsite == 4)
-    force_tile<4, 1, PREC>(d, c, t, L, rb, tile_size);
+    force_tile<4, 1, PREC>(d, c, t, tix, L, rb, tile_size);
   else
-    force_tile<5, 1, PREC>(d, c, t, L, rb, tile_size);
+    force_tile<5, 1, PREC>(d, c, t, tix, L, rb, tile_size);
 }
 
 // ------------------------------------------------------------------ per-replica kernels
@@ -1216,6 +1258,16 @@ void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, boo
     k_integrate<false><<<d.ntiles, tile, 0, s>>>(d, X, Y, prec);
 }
 size_t force_smem_bytes(int tile) { return (size_t)(3 * kMaxSites + 8) * tile * sizeof(double); }
+
+cudaError_t force_kernel_setup() {
+  // FP32 form: tiles up to 256 molecules need more than the default 48 KB of
+  // dynamic shared memory (the per-thread FP64 accumulators)
+  const int sm = (int)force_smem_bytes(256);
+  cudaError_t e = cudaFuncSetAttribute(k_force<kF32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_force<kF32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
 
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s) {

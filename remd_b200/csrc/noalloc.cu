@@ -7,7 +7,7 @@
 // cudaMalloc/cudaFree (both can synchronise the device).  They can still pass
 // in their own input and output buffers, but not give the engine its working
 // memory.  This entry point therefore keeps all of its scratch -- the
-// per-replica constants, the force records, the neighbour lists, the partial
+// per-replica constants, the force records, the neighbour lists (skin and per-step), the partial
 // sums -- in one file-scope __device__ array of fixed size, which every GPU that
 // loads the library holds until the process exits.
 //
@@ -47,7 +47,8 @@ constexpr size_t kOffPack = kOffN + al(8 * 4 * kNoAllocMaxMol);
 constexpr size_t kOffRef = kOffPack + al(4 * 20 * kNoAllocMaxMol);
 constexpr size_t kOffLb = kOffRef + al(sizeof(int4) * kNoAllocMaxMol);
 constexpr size_t kOffNbr = kOffLb + al(8 * 3 * kNoAllocMaxTiles);
-constexpr size_t kOffCnt = kOffNbr + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
+constexpr size_t kOffNbt = kOffNbr + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
+constexpr size_t kOffCnt = kOffNbt + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
 constexpr size_t kOffPart = kOffCnt + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * kNoAllocMaxTiles);
 constexpr size_t kScratchBytes = kOffErr + al(16);
@@ -188,6 +189,7 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   d.ref_com = reinterpret_cast<int4*>(b + kOffRef);
   d.Lbuild = reinterpret_cast<double*>(b + kOffLb);
   d.nbr = reinterpret_cast<uint16_t*>(b + kOffNbr);
+  d.nbt = reinterpret_cast<uint16_t*>(b + kOffNbt);
   d.nbr_cnt = reinterpret_cast<int*>(b + kOffCnt);
   d.wall = d_wall;
   d.part1 = nullptr;

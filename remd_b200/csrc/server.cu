@@ -75,7 +75,8 @@ size_t estimate_bytes(const remd_system_desc& s, int nrep) {
   int cap = ((int)std::ceil(0.1 * 4.0 / 3.0 * M_PI * rl * rl * rl) + 7) / 8 * 8;
   cap = std::min(cap, s.nmol - 1);
   const size_t ntile = (s.nmol + 127) / 128;
-  const size_t per_rep = (size_t)s.nmol * (176 + 80 + 16 + 4) + ntile * (size_t)cap * 128 * 2 +
+  // skin list + FP32 per-step list: 2 x 2 bytes per slot
+  const size_t per_rep = (size_t)s.nmol * (176 + 80 + 16 + 4) + ntile * (size_t)cap * 128 * 4 +
                          ntile * (3 * 8 + 64 + 64 + 16) + 1024;
   return per_rep * nrep + (size_t)std::max(s.nfwall, 0) * 16 + 4096;
 }

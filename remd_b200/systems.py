@@ -300,6 +300,22 @@ def feasible_periodic_length(confined, nmol, wall):
     return math.ceil(math.sqrt(nmol / nz)) * 3.1
 
 
+def feasible_geometry(rng, confined, nmol, tube_r, slit_w, rc):
+    """(confined, wall, rc) for a drawn system: a liquid-density lattice whose
+    periodic length would fall below 2*rc+2 A (the minimum-image bound) gets the
+    largest feasible rc >= 8.5 A; if none exists the system becomes a nanotube,
+    whose periodic length grows with nmol (rc redrawn, radius shrunk until it fits)."""
+    wall = tube_r if confined == 1 else slit_w if confined == 2 else 0.0
+    Lp = feasible_periodic_length(confined, nmol, wall)
+    if Lp < 2.0 * rc + 2.0:
+        rc = (Lp - 2.0) / 2.0
+        if rc < 8.5:
+            confined, wall, rc = 1, tube_r, float(rng.uniform(8.5, 12.0))
+            while feasible_periodic_length(1, nmol, wall) < 2.0 * rc + 2.0:
+                wall -= 0.25
+    return confined, wall, rc
+
+
 def config4(seed=4, interval=100):
     """8 ensembles, 256 replicas: nmol log-uniform 64-2048, models uniform over
     TIP3P/4P/5P, confinement uniform over bulk/tube (R 6-8 A)/slit (7-14 A),
@@ -322,17 +338,41 @@ def config4(seed=4, interval=100):
         slit_w = float(rng.uniform(7.0, 14.0))
         rc = float(rng.uniform(8.5, 12.0))
         drs = float(rng.choice([1.0, 2.0]))
-        wall = tube_r if confined == 1 else slit_w if confined == 2 else 0.0
-        Lp = feasible_periodic_length(confined, nmol, wall)
-        if Lp < 2.0 * rc + 2.0:
-            rc = (Lp - 2.0) / 2.0
-            if rc < 8.5:
-                confined, wall, rc = 1, tube_r, float(rng.uniform(8.5, 12.0))
-                while feasible_periodic_length(1, nmol, wall) < 2.0 * rc + 2.0:
-                    wall -= 0.25
+        confined, wall, rc = feasible_geometry(rng, confined, nmol, tube_r, slit_w, rc)
         out.append(make_ensemble(f"config4.{e}", model, confined, nmol, wall, rc, rc - drs, nt,
                                  npr, 200, 400, 0.1e6, 300e6, seed * 1000 + e, interval=interval))
     return out
+
+
+SERVING_RATE = 20.0   # mean job arrivals per second
+
+
+def config5_arrivals(seed=5, njobs=8, rate=SERVING_RATE):
+    """Poisson arrival times (s) of the serving stream."""
+    rng = np.random.default_rng([seed, 1 << 20])
+    return np.cumsum(rng.exponential(1.0 / rate, njobs))
+
+
+def config5_job(seed, k, interval=100):
+    """Job k of the serving stream: nmol log-uniform 96-4096, model uniform over
+    TIP3P/4P/5P, confinement uniform over bulk/tube (R 6-8 A)/slit (7-14 A), rc
+    8.5-12 (rs = rc-1 or rc-2), 8-64 replicas (npress 1/2/4) over 200-400 K x
+    0.1-300 MPa, interval 100, ninterval 10-200.  Returns (ensemble, ninterval)."""
+    rng = np.random.default_rng([seed, k])
+    nmol = int(round(math.exp(rng.uniform(math.log(96), math.log(4096)))))
+    model = ["tip3p", "tip4p", "tip5p"][rng.integers(3)]
+    confined = int(rng.integers(3))
+    tube_r = float(rng.uniform(6.0, 8.0))
+    slit_w = float(rng.uniform(7.0, 14.0))
+    rc = float(rng.uniform(8.5, 12.0))
+    drs = float(rng.choice([1.0, 2.0]))
+    npr = int([1, 2, 4][rng.integers(3)])
+    nt = int(rng.integers(-(-8 // npr), 64 // npr + 1))
+    ninterval = int(rng.integers(10, 201))
+    confined, wall, rc = feasible_geometry(rng, confined, nmol, tube_r, slit_w, rc)
+    ens = make_ensemble(f"config5.{k}", model, confined, nmol, wall, rc, rc - drs, nt, npr, 200,
+                        400, 0.1e6, 300e6, seed * 1000 + k, interval=interval)
+    return ens, ninterval
 
 
 def small_ensemble(model="tip4p", confined=0, nmol=64, ntemp=2, npress=2, seed=11,
