@@ -411,12 +411,24 @@ def force_accuracy(eng, ens, dev):
     ref = E.REMDGPU(ens, precision="fp64", device=dev, states=sts)
     ref.compute_forces()
     fe, ne, ue, ve = [], [], [], []
+    worst = None
+    meta = [(ei, e.spec.moltype.name, e.spec.confined, round(e.spec.rcut, 3), e.spec.nmol)
+            for ei, e in enumerate(ens) for _ in e.states]
     for k, g in enumerate(got):
         h = ref.ConvertVariablesToHost(k)
         fe.append(np.linalg.norm(g["f"] - h["f"]) / np.linalg.norm(h["f"]))
         ne.append(np.linalg.norm(g["n"] - h["n"]) / np.linalg.norm(h["n"]))
         ue.append(abs(g["pot"] - h["pot"]) / abs(h["pot"]))
         ve.append(np.linalg.norm(g["vir"] - h["vir"]) / np.linalg.norm(h["vir"]))
+        if worst is None or fe[-1] > worst[0]:
+            dm = np.linalg.norm(g["f"] - h["f"], axis=1)
+            i = int(np.argmax(dm))
+            worst = (fe[-1], {"replica": k, "ensemble": meta[k][0], "model": meta[k][1],
+                              "confined": meta[k][2], "rcut": meta[k][3], "nmol": meta[k][4],
+                              "box": [float(x) for x in h["L"]], "molecule": i,
+                              "abs_err": float(dm[i]),
+                              "force_abs": float(np.linalg.norm(h["f"][i])),
+                              "force_abs_median": float(np.median(np.linalg.norm(h["f"], axis=1)))})
     ref.close()
     return {"reference": "FP64 form of this engine on the same snapshots",
             "replicas": len(got),
@@ -424,6 +436,8 @@ def force_accuracy(eng, ens, dev):
             "torque_rms_rel_max": float(max(ne)),
             "pot_rel_max": float(max(ue)), "pot_rel_median": float(np.median(ue)),
             "virial_rel_max": float(max(ve)),
+            "replicas_over_force_gate": int(sum(1 for x in fe if x > 1e-5)),
+            "worst": worst[1],
             "gates": {"force_rms_rel": 1e-5, "pot_rel": 1e-6}}
 
 

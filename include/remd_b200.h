@@ -191,7 +191,7 @@ remd_status remd_measure_fp32_peak(int device, double *tflops);
 /* Per-replica health word of the last interval: 0 ok, else a remd_status. */
 remd_status remd_replica_status(remd_handle h, int rep, int *status);
 
-/* Tuning: atoms of one force tile (32..256, multiple of 32) and the neighbour
+/* Tuning: molecules of one force tile (32..128, multiple of 32) and the neighbour
  * skin (A).  Takes effect on the next call. */
 remd_status remd_set_tuning(remd_handle h, int tile, double skin);
 

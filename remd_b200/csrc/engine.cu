@@ -558,8 +558,8 @@ remd_status remd_destroy(remd_handle h) {
 }
 
 remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
-  if (!h || tile < 32 || tile > 256 || tile % 32 || !(skin > 0.0)) {
-    set_error("remd_set_tuning: tile must be 32..256 (multiple of 32), skin > 0");
+  if (!h || tile < 32 || tile > 128 || tile % 32 || !(skin > 0.0)) {
+    set_error("remd_set_tuning: tile must be 32..128 (multiple of 32), skin > 0");
     return REMD_ERR_INVALID;
   }
   if (tile == h->tile && skin == h->skin) return REMD_OK;

@@ -4,6 +4,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "integrator.cuh"
 #include "kernels.cuh"
 
@@ -306,24 +308,110 @@ struct IAcc {
 
 // FP32 pair loop over i's neighbour list, in two passes.
 // Pass 1 scans the (rcut + skin) list and writes the neighbours within rcut, in
-// the list's ascending-j order, to i's column of the per-step list `nbt`
-// (same layout and capacity as the skin list; it cannot overflow).  Pass 2
-// computes exactly those pairs, so the lanes of a warp stay converged (no
-// cutoff branch) and differ only in their pair counts.
+// the list's ascending-j order, to i's column of the per-step list `nbt` (same
+// layout and capacity as the skin list; it cannot overflow).  Under the
+// per-site minimum image (SIMG, below) it splits them: pairs whose COM vector
+// keeps every site-pair component clear of +-L/2 ("far", from the front of the
+// column) need no per-site image at all; the others ("near", from the back)
+// get the per-site image.  Pass 2 computes exactly those pairs, so the lanes of
+// a warp stay converged (no cutoff branch) and differ only in their counts.
 // Pair math in FP32 (rsqrt on the SFU plus one Newton step); partial sums in
-// FP32 over 8 pairs, then FP64 accumulation into this thread's slots of `acc`
+// FP32 over 16 pairs, then FP64 accumulation into this thread's slots of `acc`
 // (shared memory, field f at acc[f * blockDim.x + threadIdx.x]: 3S site-force
 // components, 3 switching-correction, 3 virial, LJ, Coulomb).  The pairs within
-// rcut, in ascending j, and their grouping by 8 depend only on the positions,
-// not on when the skin list was built.  Neighbour indices are read two pairs
-// ahead and records one pair ahead of their use.
+// rcut, their far/near class and order, and their grouping by 16 depend only
+// on the positions, not on when the skin list was built.  Neighbour indices
+// are read two pairs ahead and records one pair ahead of their use.
 // SIMG: apply the minimum image to every site pair as the reference does
 // (src/force_calculator.cxx:737-741).  It changes the result only when a box
 // length is below 2 (rc + 2 site_reach); the caller enables it just then.
 struct F32Const {
   float qq[kMaxSites][kMaxSites];
   float Ls[3], Lf[3], hL[3];
+  double L[3];
 };
+
+// Per-site minimum image (SIMG) flips a site-pair vector by a box length where
+// one of its components crosses +-L/2, so the FP32 and FP64 forms must take the
+// same image there.  A site pair with a component within kImageTol of L/2
+// (FP32 rounding of the site vector is below ~4e-6 A) is left out of the pair
+// loop (its vector is set far away, so its terms vanish) and added afterwards
+// by site_pair_exact: the image is decided with the FP64 form's arithmetic
+// (pair_loop_f64: COM vector from the FP64 box fractions, site offsets R(q) b
+// in FP64), then the terms are evaluated as in the loop.  Up to kMaxDefer such
+// site pairs per molecule and step are deferred; further ones (never seen in
+// practice) keep the FP32 image.
+constexpr float kImageTol = 2e-5f;
+constexpr int kMaxDefer = 2;
+
+template <int S, int C0>
+__device__ __noinline__ void site_pair_exact(const DevPtrs& d, const RepConst& c, const F32Const& k32, int li,
+                                             int code, double* acc) {
+  const int j = code >> 8, kk = (code >> 4) & 15, l = code & 15;
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int N = d.N, gi = c.mol_off + li, gj = c.mol_off + j;
+  const double* L = k32.L;
+  // COM vector and switch exactly as the FP32 loop forms them
+  const uint32_t* base = reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off;
+  const int stride = c.pack_stride;
+  const int* wi = reinterpret_cast<const int*>(base + (long long)li * stride);
+  const int* wj = reinterpret_cast<const int*>(base + (long long)j * stride);
+  const float dx = (float)(int)(wi[0] - wj[0]) * k32.Ls[0];
+  const float dy = (float)(int)(wi[1] - wj[1]) * k32.Ls[1];
+  const float dz = (float)(int)(wi[2] - wj[2]) * k32.Ls[2];
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2);
+  const float r = r2 * rinv;
+  const float rc = (float)c.rc, rs = (float)c.rs, coef = (float)c.coef_sw;
+  float sw = 1.f, dsw = 0.f;
+  if (r > rs) {
+    const float r01c = r - rc, r01l = r - rs;
+    sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
+    dsw = coef * 30.f * r01c * r01c * r01l * r01l;
+  }
+  // the site vector with the FP64 form's image
+  double qi[4], qj[4], si[3], sj[3];
+  for (int x = 0; x < 4; x++) { qi[x] = d.q[x * N + gi]; qj[x] = d.q[x * N + gj]; }
+  body_to_space(qi, c.body[kk], si);
+  body_to_space(qj, c.body[l], sj);
+  float v[3];
+  for (int x = 0; x < 3; x++) {
+    double gr = (d.r[x * N + gi] - d.r[x * N + gj]) * L[x];
+    if (gr >= 0.5 * L[x]) gr -= L[x];
+    if (gr < -0.5 * L[x]) gr += L[x];
+    double rv = gr + si[x] - sj[x];
+    if (rv >= 0.5 * L[x]) rv -= L[x];
+    if (rv < -0.5 * L[x]) rv += L[x];
+    v[x] = (float)rv;
+  }
+  const float rr = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  float ri = rsqrtf(rr);
+  ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);
+  const float ri2 = ri * ri;
+  float ftmp = 0.f, elj = 0.f, ecl = 0.f;
+  if (kk == 0 && l == 0) {
+    float s6 = (float)c.sgm2 * ri2;
+    s6 = s6 * s6 * s6;
+    elj = (float)(4.0 * c.eps) * s6 * (s6 - 1.f);
+    ftmp += (float)(48.0 * c.eps) * s6 * (s6 - 0.5f) * ri2;
+  }
+  if (kk >= C0 && l >= C0) {
+    ecl = k32.qq[kk][l] * ri;
+    ftmp += ecl * ri2;
+  }
+  ftmp *= sw;
+  const float t[3] = {v[0] * ftmp, v[1] * ftmp, v[2] * ftmp};
+  const float g = dsw * rinv * (elj + ecl);
+  const float cv[3] = {-dx * g, -dy * g, -dz * g};
+  const float dv[3] = {dx, dy, dz};
+  for (int x = 0; x < 3; x++) {
+    acc[(3 * kk + x) * T + tid] += (double)t[x];
+    acc[(3 * S + x) * T + tid] += (double)cv[x];
+    acc[(3 * S + 3 + x) * T + tid] += (double)((t[x] + cv[x]) * dv[x]);
+  }
+  acc[(3 * S + 6) * T + tid] += (double)(sw * elj);
+  acc[(3 * S + 7) * T + tid] += (double)(sw * ecl);
+}
 
 template <int S, int C0, bool SIMG>
 __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const F32Const& k32,
@@ -350,9 +438,27 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 #pragma unroll
       for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
   }
+  // far bound: |d_x| below it keeps every site-pair component below L/2 - kImageTol
+  float bnd0 = 0.f, bnd1 = 0.f, bnd2 = 0.f;
+  if (SIMG) {
+    const float m = 2.f * (float)c.site_reach + kImageTol + 1e-3f;
+    bnd0 = k32.hL[0] - m; bnd1 = k32.hL[1] - m; bnd2 = k32.hL[2] - m;
+  }
+  const int back = c.nbr_cap - 1;
   // pass 1: neighbours within rcut (same FP32 distance as pass 2), eight
   // candidates per round so that their loads are in flight together
-  int np = 0;
+  int nfar = 0, nnear = 0;
+  auto keep = [&](int j, float dx, float dy, float dz) {
+    if (dx * dx + dy * dy + dz * dz <= rc2) {
+      if (SIMG && (fabsf(dx) >= bnd0 || fabsf(dy) >= bnd1 || fabsf(dz) >= bnd2)) {
+        nt[(long long)(back - nnear) * T] = (uint16_t)j;
+        nnear++;
+      } else {
+        nt[(long long)nfar * T] = (uint16_t)j;
+        nfar++;
+      }
+    }
+  };
   {
     constexpr int B = 8;
     int k = 0;
@@ -364,33 +470,20 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 #pragma unroll
       for (int m = 0; m < B; m++) u[m] = __ldg(base + (long long)j[m] * NV);
 #pragma unroll
-      for (int m = 0; m < B; m++) {
-        const float dx = (float)(int)(xi - (int)u[m].x) * Ls0;
-        const float dy = (float)(int)(yi - (int)u[m].y) * Ls1;
-        const float dz = (float)(int)(zi - (int)u[m].z) * Ls2;
-        if (dx * dx + dy * dy + dz * dz <= rc2) {
-          nt[(long long)np * T] = (uint16_t)j[m];
-          np++;
-        }
-      }
+      for (int m = 0; m < B; m++)
+        keep(j[m], (float)(int)(xi - (int)u[m].x) * Ls0, (float)(int)(yi - (int)u[m].y) * Ls1,
+             (float)(int)(zi - (int)u[m].z) * Ls2);
     }
     for (; k < cnt; k++) {
       const int j = nb[(long long)k * T];
       const uint4 u = __ldg(base + (long long)j * NV);
-      const float dx = (float)(int)(xi - (int)u.x) * Ls0;
-      const float dy = (float)(int)(yi - (int)u.y) * Ls1;
-      const float dz = (float)(int)(zi - (int)u.z) * Ls2;
-      if (dx * dx + dy * dy + dz * dz <= rc2) {
-        nt[(long long)np * T] = (uint16_t)j;
-        np++;
-      }
+      keep(j, (float)(int)(xi - (int)u.x) * Ls0, (float)(int)(yi - (int)u.y) * Ls1,
+           (float)(int)(zi - (int)u.z) * Ls2);
     }
   }
   const float rc = (float)c.rc, rs = (float)c.rs;
   const float coef = (float)c.coef_sw;
   const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
-  const float hL0 = k32.hL[0], hL1 = k32.hL[1], hL2 = k32.hL[2];
-  const float Lf0 = k32.Lf[0], Lf1 = k32.Lf[1], Lf2 = k32.Lf[2];
 
   float fs[S][3], fc[3], fv[3], flj, fcl;
   auto zero = [&]() {
@@ -414,96 +507,122 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
     acc[(3 * S + 7) * T + tid] += (double)fcl;
   };
   zero();
-  // pass 2: the pairs within rcut
-  uint4 nx[NV];
-  int jnext = (np > 1) ? nt[T] : 0;
-  if (np > 0) {
-    const int j0 = nt[0];
+  int done = 0;                       // pairs accumulated (partial sums close every 16)
+  int ndef = 0, def0 = 0, def1 = 0;   // deferred site pairs (near pass only)
+
+  // pass 2: `n` pairs of the list starting at column slot `pos0`, stepping `dir`;
+  // IMG: per-site minimum image with exact ties (near pairs)
+  auto run = [&](auto img, int n, int pos0, int dir) {
+    constexpr bool IMG = decltype(img)::value;
+    const float hL0 = k32.hL[0], hL1 = k32.hL[1], hL2 = k32.hL[2];
+    const float Lf0 = k32.Lf[0], Lf1 = k32.Lf[1], Lf2 = k32.Lf[2];
+    uint4 nx[NV];
+    int jnext = (n > 1) ? nt[(long long)(pos0 + dir) * T] : 0;
+    int jpre = 0;
+    if (n > 0) {
+      const int j0 = nt[(long long)pos0 * T];
+      jpre = j0;
 #pragma unroll
-    for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)j0 * NV + m);
-  }
-  for (int k = 0; k < np; k++) {
-    uint32_t wj[STRIDE];
-#pragma unroll
-    for (int m = 0; m < NV; m++) {
-      wj[4 * m] = nx[m].x; wj[4 * m + 1] = nx[m].y; wj[4 * m + 2] = nx[m].z; wj[4 * m + 3] = nx[m].w;
+      for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)j0 * NV + m);
     }
-    if (k + 1 < np) {
-      const int jn = jnext;
-      if (k + 2 < np) jnext = nt[(long long)(k + 2) * T];
+    for (int k = 0; k < n; k++) {
+      uint32_t wj[STRIDE];
 #pragma unroll
-      for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
-    }
-    const float dx = (float)(int)(xi - (int)wj[0]) * Ls0;
-    const float dy = (float)(int)(yi - (int)wj[1]) * Ls1;
-    const float dz = (float)(int)(zi - (int)wj[2]) * Ls2;
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    const float rinv = rsqrtf(r2);
-    const float r = r2 * rinv;
-    float sw = 1.f, dsw = 0.f;
-    if (r > rs) {
-      const float r01c = r - rc, r01l = r - rs;
-      sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
-      dsw = coef * 30.f * r01c * r01c * r01l * r01l;
-    }
-    float elj = 0.f, ecl = 0.f;
-    float fpx = 0.f, fpy = 0.f, fpz = 0.f;
-#pragma unroll
-    for (int kk = 0; kk < S; kk++) {
-      if (kk != 0 && kk < C0) continue;
-      const float ax = dx + si[kk][0], ay = dy + si[kk][1], az = dz + si[kk][2];
-      float tx = 0.f, ty = 0.f, tz = 0.f;
-#pragma unroll
-      for (int l = 0; l < S; l++) {
-        const bool lj_pair = (kk == 0 && l == 0);
-        const bool cl_pair = (kk >= C0 && l >= C0);
-        if (!lj_pair && !cl_pair) continue;
-        float x = ax - __uint_as_float(wj[3 + 3 * l]);
-        float y = ay - __uint_as_float(wj[3 + 3 * l + 1]);
-        float z = az - __uint_as_float(wj[3 + 3 * l + 2]);
-        if (SIMG) {
-          if (x >= hL0) x -= Lf0;
-          if (x < -hL0) x += Lf0;
-          if (y >= hL1) y -= Lf1;
-          if (y < -hL1) y += Lf1;
-          if (z >= hL2) z -= Lf2;
-          if (z < -hL2) z += Lf2;
-        }
-        const float rr = x * x + y * y + z * z;
-        float ri = rsqrtf(rr);
-        ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);   // one Newton step: ~0.5 ulp
-        const float ri2 = ri * ri;
-        float ftmp = 0.f;
-        if (lj_pair) {
-          float s6 = sgm2 * ri2;
-          s6 = s6 * s6 * s6;
-          elj += eps4 * s6 * (s6 - 1.f);
-          ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
-        }
-        if (cl_pair) {
-          const float e = k32.qq[kk][l] * ri;
-          ecl += e;
-          ftmp += e * ri2;
-        }
-        ftmp *= sw;
-        tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
+      for (int m = 0; m < NV; m++) {
+        wj[4 * m] = nx[m].x; wj[4 * m + 1] = nx[m].y; wj[4 * m + 2] = nx[m].z; wj[4 * m + 3] = nx[m].w;
       }
-      fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
-      fpx += tx; fpy += ty; fpz += tz;
+      const int jcur = jpre;
+      if (k + 1 < n) {
+        const int jn = jnext;
+        jpre = jn;
+        if (k + 2 < n) jnext = nt[(long long)(pos0 + dir * (k + 2)) * T];
+#pragma unroll
+        for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
+      }
+      const float dx = (float)(int)(xi - (int)wj[0]) * Ls0;
+      const float dy = (float)(int)(yi - (int)wj[1]) * Ls1;
+      const float dz = (float)(int)(zi - (int)wj[2]) * Ls2;
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      const float rinv = rsqrtf(r2);
+      const float r = r2 * rinv;
+      float sw = 1.f, dsw = 0.f;
+      if (r > rs) {
+        const float r01c = r - rc, r01l = r - rs;
+        sw = coef * r01c * r01c * r01c * (10.f * r01l * r01l - 5.f * r01l * r01c + r01c * r01c);
+        dsw = coef * 30.f * r01c * r01c * r01l * r01l;
+      }
+      float elj = 0.f, ecl = 0.f;
+      float fpx = 0.f, fpy = 0.f, fpz = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < S; kk++) {
+        if (kk != 0 && kk < C0) continue;
+        const float ax = dx + si[kk][0], ay = dy + si[kk][1], az = dz + si[kk][2];
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+        for (int l = 0; l < S; l++) {
+          const bool lj_pair = (kk == 0 && l == 0);
+          const bool cl_pair = (kk >= C0 && l >= C0);
+          if (!lj_pair && !cl_pair) continue;
+          float x = ax - __uint_as_float(wj[3 + 3 * l]);
+          float y = ay - __uint_as_float(wj[3 + 3 * l + 1]);
+          float z = az - __uint_as_float(wj[3 + 3 * l + 2]);
+          if (IMG) {
+            if ((fabsf(fabsf(x) - hL0) < kImageTol || fabsf(fabsf(y) - hL1) < kImageTol ||
+                 fabsf(fabsf(z) - hL2) < kImageTol) && ndef < kMaxDefer) {
+              const int code = (jcur << 8) | (kk << 4) | l;
+              if (ndef == 0) def0 = code; else def1 = code;
+              ndef++;
+              x = y = z = 1e18f;   // this site pair's terms vanish here; added exactly below
+            }
+            if (x >= hL0) x -= Lf0;
+            if (x < -hL0) x += Lf0;
+            if (y >= hL1) y -= Lf1;
+            if (y < -hL1) y += Lf1;
+            if (z >= hL2) z -= Lf2;
+            if (z < -hL2) z += Lf2;
+          }
+          const float rr = x * x + y * y + z * z;
+          float ri = rsqrtf(rr);
+          ri = ri * fmaf(-0.5f * rr * ri, ri, 1.5f);   // one Newton step: ~0.5 ulp
+          const float ri2 = ri * ri;
+          float ftmp = 0.f;
+          if (lj_pair) {
+            float s6 = sgm2 * ri2;
+            s6 = s6 * s6 * s6;
+            elj += eps4 * s6 * (s6 - 1.f);
+            ftmp += eps48 * s6 * (s6 - 0.5f) * ri2;
+          }
+          if (cl_pair) {
+            const float e = k32.qq[kk][l] * ri;
+            ecl += e;
+            ftmp += e * ri2;
+          }
+          ftmp *= sw;
+          tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
+        }
+        fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
+        fpx += tx; fpy += ty; fpz += tz;
+      }
+      const float e = elj + ecl;
+      const float g = dsw * rinv * e;
+      const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
+      fc[0] += cx; fc[1] += cy; fc[2] += cz;
+      fv[0] += (fpx + cx) * dx;
+      fv[1] += (fpy + cy) * dy;
+      fv[2] += (fpz + cz) * dz;
+      flj += sw * elj;
+      fcl += sw * ecl;
+      if ((++done & 15) == 0) { flush(); zero(); }
     }
-    const float e = elj + ecl;
-    const float g = dsw * rinv * e;
-    const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
-    fc[0] += cx; fc[1] += cy; fc[2] += cz;
-    fv[0] += (fpx + cx) * dx;
-    fv[1] += (fpy + cy) * dy;
-    fv[2] += (fpz + cz) * dz;
-    flj += sw * elj;
-    fcl += sw * ecl;
-    if ((k & 15) == 15) { flush(); zero(); }
-  }
+  };
+  run(std::false_type{}, nfar, 0, 1);
+  if (SIMG) run(std::true_type{}, nnear, back, -1);
   flush();
-  npair += np;
+  if (SIMG && ndef > 0) {
+    site_pair_exact<S, C0>(d, c, k32, li, def0, acc);
+    if (ndef > 1) site_pair_exact<S, C0>(d, c, k32, li, def1, acc);
+  }
+  npair += nfar + nnear;
 }
 
 template <int S, int C0, bool SIMG>
@@ -622,6 +741,7 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, i
         k32.Ls[x] = (float)(L[x] * kFixInv);
         k32.Lf[x] = (float)L[x];
         k32.hL[x] = 0.5f * (float)L[x];
+        k32.L[x] = L[x];
       }
     }
     for (int f = 0; f < 3 * S + 8; f++) acc[f * T + i] = 0.0;
@@ -720,7 +840,7 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, i
 }
 
 template <int PREC, bool FORCE_ONLY>
-__global__ void __launch_bounds__(256) k_force(DevPtrs d, const RepState* __restrict__ Yin,
+__global__ void __launch_bounds__(128, PREC == kF32 ? 3 : 1) k_force(DevPtrs d, const RepState* __restrict__ Yin,
                                                RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
   const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;   // costliest tiles first
@@ -1260,9 +1380,10 @@ void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, boo
 size_t force_smem_bytes(int tile) { return (size_t)(3 * kMaxSites + 8) * tile * sizeof(double); }
 
 cudaError_t force_kernel_setup() {
-  // FP32 form: tiles up to 256 molecules need more than the default 48 KB of
-  // dynamic shared memory (the per-thread FP64 accumulators)
-  const int sm = (int)force_smem_bytes(256);
+  // FP32 form: dynamic shared memory = the per-thread FP64 accumulators of a tile
+  // of up to 128 molecules (23.5 KB, under the default limit; set explicitly so
+  // that a larger tile or more accumulators only change force_smem_bytes)
+  const int sm = (int)force_smem_bytes(128);
   cudaError_t e = cudaFuncSetAttribute(k_force<kF32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_force<kF32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);

@@ -8,6 +8,8 @@ Tolerances (relative L2 norms over all molecules unless stated):
   20-step trajectories (chaotic, errors grow ~e^(t/tau)): FP64 1e-8, FP32 see
   the per-quantity bounds in test_twenty_steps.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -288,6 +290,34 @@ def test_fp32_accuracy_tip5p_bulk_1728():
     assert rel(g["f"], orc.f) < 1e-5
     assert rel(g["n"], orc.n) < 1e-5
     assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
+
+
+def _simg_tie_case():
+    z = np.load(os.path.join(GOLDEN, "simg_tie.npz"))
+    e = S.make_ensemble("tie", "tip3p", 0, len(z["r"]), 0.0, float(z["rcut"]), float(z["rswitch"]),
+                        1, 1, 300, 300, 0.1e6, 0.1e6, 4)
+    st = e.states[0]
+    st.r, st.q, st.L = z["r"].copy(), z["q"].copy(), z["L"].copy()
+    st.v[:] = 0.0
+    st.p[:] = 0.0
+    return e.spec, st, z["ties"]
+
+
+def test_fp32_site_image_ties_follow_oracle():
+    """Site pairs with a component within 1e-7..3e-6 A of L/2 under the per-site
+    minimum image (src/force_calculator.cxx:737-741): the FP32 form takes the
+    oracle's image for each, so no site force flips direction."""
+    spec, st, ties = _simg_tie_case()
+    eng = E.REMDGPU([single(spec, st)], precision="fp32")
+    g = eng.ConvertVariablesToHost(0)
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    assert rel(g["f"], orc.f) < 1e-5
+    assert rel(g["n"], orc.n) < 1e-5
+    scale = np.median(np.linalg.norm(orc.f, axis=1))
+    for i, j, _, _, _ in ties:
+        for m in (i, j):
+            assert np.linalg.norm(g["f"][m] - orc.f[m]) < 1e-5 * scale * 10
 
 
 def test_graph_exchange_equals_explicit_exchange():

@@ -53,3 +53,20 @@ def test_config4_shape():
         assert e.spec.moltype.nsite in (3, 4, 5)
         assert 8.5 <= e.spec.rcut <= 12.0
         assert e.spec.rcut - e.spec.rswitch in (1.0, 2.0)
+
+
+def test_simg_tie_fixture_offsets():
+    """The committed site-image tie configuration holds the ties it claims:
+    |x| - L/2 for each listed site pair, recomputed in FP64."""
+    import os
+    from tests.common import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "simg_tie.npz"))
+    b = S.load_model("tip3p").r
+    r, q, L = z["r"], z["q"], z["L"]
+    for (i, j, k, l, ax), off in zip(z["ties"], z["offsets"]):
+        gr = (r[i] - r[j]) * L
+        gr = np.where(gr >= 0.5 * L, gr - L, gr)
+        gr = np.where(gr < -0.5 * L, gr + L, gr)
+        rv = gr + S.body_to_space(q[i:i + 1], b)[0, k] - S.body_to_space(q[j:j + 1], b)[0, l]
+        assert abs(rv[ax]) - 0.5 * L[ax] == pytest.approx(off, abs=1e-9)
+        assert 1e-8 < abs(off) < 4e-6
