@@ -57,8 +57,8 @@ def parse_args(argv=None):
     ap.add_argument("--jobs", type=int, default=8, help="config 5: jobs of the serving stream")
     ap.add_argument("--budget-gib", type=float, default=24.0, help="config 5: server HBM budget")
     ap.add_argument("--interval", type=int, default=100)
-    ap.add_argument("--tile", type=int, default=128)
-    ap.add_argument("--skin", type=float, default=1.0)
+    ap.add_argument("--tile", type=int, default=0, help="force tile (0: autotuned)")
+    ap.add_argument("--skin", type=float, default=0.0, help="neighbour skin in A (0: autotuned)")
     ap.add_argument("--seed", type=int, default=None, help="workload seed (default: the config index)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -451,8 +451,8 @@ def engine_arm(args, rank, world, local):
     torch.cuda.set_device(dev)
     ens = rank_workload(args, rank)
     eng = E.REMDGPU(ens, precision="fp32", device=dev)
-    if args.tile != 128 or args.skin != 1.0:
-        eng.set_tuning(args.tile, args.skin)
+    if args.tile or args.skin:
+        eng.set_tuning(args.tile or 128, args.skin or 1.0)
     T = np.concatenate([e.T for e in ens])
     P = np.concatenate([e.P for e in ens])
     nmol_total = int(sum(e.spec.nmol for e in ens for _ in e.states))
@@ -461,6 +461,13 @@ def engine_arm(args, rank, world, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
     # untimed: relax the lattice start (init_scaling every 20 steps), then warm up
     eng.equilibrate(rounds=args.equil_rounds, steps=20)
+    # untimed: the autotuner picks (tile, skin) on this batch; the trajectory does
+    # not depend on the choice
+    if args.tile or args.skin:
+        tuning = {"tile": args.tile or 128, "skin": args.skin or 1.0, "autotuned": False}
+    else:
+        t, k, tms = eng.autotune(nsteps=20)
+        tuning = {"tile": t, "skin": k, "autotuned": True, "ms_per_md_step": tms}
     # one bench step = one REMD interval: `interval` MD steps of every replica and
     # the Metropolis exchange of every ensemble, all on the device
     eng.enable_device_exchange([(e.ntemp, e.npress) for e in ens], seed=2024 + rank)
@@ -579,7 +586,7 @@ def engine_arm(args, rank, world, local):
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": workload_desc(args.config, ens, args.interval),
+                "config": dict(workload_desc(args.config, ens, args.interval), tuning=tuning),
                 "gpu_launches": eng.launches_per_interval() * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "latency": {"p50_interval_ms": float(np.percentile(ms, 50)),

@@ -195,6 +195,15 @@ remd_status remd_replica_status(remd_handle h, int rep, int *status);
  * skin (A).  Takes effect on the next call. */
 remd_status remd_set_tuning(remd_handle h, int tile, double skin);
 
+/* Autotuner (no counterpart in the reference): times every (tile, skin) of
+ * {32, 64, 96, 128} x {0.6, 0.8, 1.0, 1.4} A over `nsteps` MD steps of this
+ * batch (integrate + force per step, CUDA events), restores the state after
+ * each trial and keeps the fastest.  The trajectory does not depend on the
+ * choice: forces are a function of positions only and every partial sum is
+ * per 32 molecules.  Outputs (any may be NULL): the chosen tile, skin and its
+ * ms per MD step.  Synchronous; call it before stream capture. */
+remd_status remd_autotune(remd_handle h, int nsteps, int *tile, double *skin, double *ms_per_step);
+
 /* ---- exchange (src/remd.cxx:467-538, src/remdinfo.cxx:54-125) ------------- */
 
 /* REMD::ReplicaExchange for one ensemble on the host: index (condition slot ->

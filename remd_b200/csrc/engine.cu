@@ -105,10 +105,14 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
   const int T = h->tile;
   h->tiles.clear();
   long long pack_words = 0, nbr_words = 0;
+  int nwarps = 0;
   for (int r = 0; r < h->nrep; r++) {
     RepConst& c = h->rc[r];
     c.tile_off = (int)h->tiles.size();
     c.ntile = (c.nmol + T - 1) / T;
+    c.warp_off = nwarps;
+    c.nwarp = (c.nmol + 31) / 32;
+    nwarps += c.nwarp;
     for (int t = 0; t < c.ntile; t++) {
       Tile tt;
       tt.rep = r;
@@ -150,7 +154,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       (size_t)nbr_words * 2,           // 11 nbr
       N * 4,                           // 12 nbr_cnt
       std::max<size_t>(h->wall_h.size(), 2) * 8,   // 13 wall
-      nt * sizeof(Part1), nt * sizeof(Part2),      // 14, 15
+      (size_t)nwarps * sizeof(Part1), (size_t)nwarps * sizeof(Part2),   // 14, 15 (per 32 molecules)
       nr * kNumAvg * 8,                // 16 avg
       nr * 4, 64,                      // 17 status, 18 err
       nr * 8, nr * 8,                  // 19 T, 20 P
@@ -303,7 +307,8 @@ static remd_status build_graph(remd_engine_s* h) {
 }
 
 static long long host_pairs(remd_engine_s* h) {
-  std::vector<Part2> p2(h->tiles.size());
+  const RepConst& last = h->rc.back();
+  std::vector<Part2> p2((size_t)last.warp_off + last.nwarp);
   if (cudaMemcpy(p2.data(), h->d.part2, p2.size() * sizeof(Part2), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;
   long long s = 0;
@@ -461,7 +466,7 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
       double qr[kMaxSites];
       for (int k = 0; k < s.nsite; k++) {
         for (int x = 0; x < 3; x++) c.body[k][x] = s.site_r[k][x] * (1e-10 / unit_length());
-        qr[k] = s.site_charge[k] * (1.6021761e-19 / unit_coulomb());
+        qr[k] = s.site_charge[k] * (elementary_charge() / unit_coulomb());
       }
       for (int k = 0; k < s.nsite; k++)
         for (int l = 0; l < s.nsite; l++) c.qq[k][l] = qr[k] * qr[l];
@@ -557,27 +562,41 @@ remd_status remd_destroy(remd_handle h) {
   return REMD_OK;
 }
 
-remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
-  if (!h || tile < 32 || tile > 128 || tile % 32 || !(skin > 0.0)) {
-    set_error("remd_set_tuning: tile must be 32..128 (multiple of 32), skin > 0");
-    return REMD_ERR_INVALID;
-  }
-  if (tile == h->tile && skin == h->skin) return REMD_OK;
-  // re-lay out the arrays for the new tile, preserving state
+// Everything a re-layout must carry: the molecule and replica state, the
+// conditions and index, and the device-exchange configuration.
+struct SavedState {
+  std::vector<double> r, v, q, p, dT, dP;
+  std::vector<RepState> st;
+  std::vector<int> idx, grid, uoff;
+  std::vector<long long> step;
+  std::vector<unsigned long long> seed;
+};
+
+static remd_status save_state(remd_engine_s* h, SavedState& sv) {
   const int N = h->N;
-  std::vector<double> r((size_t)N * 3), v((size_t)N * 3), q((size_t)N * 4), p((size_t)N * 4), f((size_t)N * 3), n((size_t)N * 4);
-  std::vector<RepState> st(h->nrep);
-  std::vector<double> dT(h->nrep), dP(h->nrep);
-  std::vector<int> idx(h->nrep);
+  sv.r.resize((size_t)N * 3); sv.v.resize((size_t)N * 3); sv.q.resize((size_t)N * 4); sv.p.resize((size_t)N * 4);
+  sv.st.resize(h->nrep); sv.dT.resize(h->nrep); sv.dP.resize(h->nrep); sv.idx.resize(h->nrep);
+  sv.grid.resize(2 * h->nens); sv.uoff.resize(h->nens); sv.step.resize(h->nens); sv.seed.resize(h->nens);
   CK(cudaStreamSynchronize(h->stream));
-  CK(cudaMemcpy(r.data(), h->d.r, r.size() * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(v.data(), h->d.v, v.size() * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(q.data(), h->d.q, q.size() * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(p.data(), h->d.p, p.size() * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(st.data(), h->X, st.size() * sizeof(RepState), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(dT.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(dP.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.r.data(), h->d.r, sv.r.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.v.data(), h->d.v, sv.v.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.q.data(), h->d.q, sv.q.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.p.data(), h->d.p, sv.p.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.st.data(), h->X, sv.st.size() * sizeof(RepState), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.dT.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.dP.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.grid.data(), h->d_grid, sv.grid.size() * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.uoff.data(), h->d_u_off, sv.uoff.size() * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.step.data(), h->d_step, sv.step.size() * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sv.seed.data(), h->d_seed, sv.seed.size() * 8, cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+// Re-lay out the arrays for (tile, skin) and restore `sv`.  Forces are a pure
+// function of the positions and every partial sum is per 32 molecules, so the
+// trajectory that follows does not depend on the tile or the skin.
+static remd_status relayout(remd_engine_s* h, int tile, double skin, const SavedState& sv) {
   h->tile = tile;
   h->skin = skin;
   for (auto& c : h->rc) {
@@ -589,19 +608,59 @@ remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
   remd_status s = allocate(h);
   if (s != REMD_OK) return s;
-  if ((s = upload_state(h, r, v, q, p, st)) != REMD_OK) return s;
+  if ((s = upload_state(h, sv.r, sv.v, sv.q, sv.p, sv.st)) != REMD_OK) return s;
   CK(cudaStreamSynchronize(h->stream));
   std::vector<int> roff(h->nens);
   for (int e = 0; e < h->nens; e++) roff[e] = h->ens_rep_off[e];
-  CK(cudaMemcpy(h->dT, dT.data(), h->nrep * 8, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->dP, dP.data(), h->nrep * 8, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->d_index, idx.data(), h->nrep * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->dT, sv.dT.data(), h->nrep * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->dP, sv.dP.data(), h->nrep * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_index, sv.idx.data(), h->nrep * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_rep_off, roff.data(), roff.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_grid, sv.grid.data(), sv.grid.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_u_off, sv.uoff.data(), sv.uoff.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_step, sv.step.data(), sv.step.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_seed, sv.seed.data(), sv.seed.size() * 8, cudaMemcpyHostToDevice));
   // forces are a pure function of positions: recompute, keep H0
   launch_pack(h->d, h->prec, h->tile, h->stream);
   launch_force(h->d, h->X, h->X, h->prec, true, h->tile, h->stream);
   CK(cudaGetLastError());
   return sync_and_check(h);
+}
+
+remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
+  if (!h || tile < 32 || tile > 128 || tile % 32 || !(skin > 0.0)) {
+    set_error("remd_set_tuning: tile must be 32..128 (multiple of 32), skin > 0");
+    return REMD_ERR_INVALID;
+  }
+  if (tile == h->tile && skin == h->skin) return REMD_OK;
+  SavedState sv;
+  remd_status s = save_state(h, sv);
+  if (s != REMD_OK) return s;
+  return relayout(h, tile, skin, sv);
+}
+
+remd_status remd_autotune(remd_handle h, int nsteps, int* tile_out, double* skin_out, double* ms_out) {
+  if (!h || nsteps < 1) return REMD_ERR_INVALID;
+  SavedState sv;
+  remd_status s = save_state(h, sv);
+  if (s != REMD_OK) return s;
+  static const int tiles[] = {32, 64, 96, 128};
+  static const double skins[] = {0.6, 0.8, 1.0, 1.4};
+  int best_tile = h->tile;
+  double best_skin = h->skin, best_ms = 1e300;
+  for (int t : tiles)
+    for (double k : skins) {
+      if ((s = relayout(h, t, k, sv)) != REMD_OK) return s;
+      double ms[2];
+      if ((s = remd_profile_steps(h, nsteps, ms)) != REMD_OK) return s;
+      const double step_ms = ms[0] + ms[1];
+      if (step_ms < best_ms) { best_ms = step_ms; best_tile = t; best_skin = k; }
+    }
+  if ((s = relayout(h, best_tile, best_skin, sv)) != REMD_OK) return s;
+  if (tile_out) *tile_out = best_tile;
+  if (skin_out) *skin_out = best_skin;
+  if (ms_out) *ms_out = best_ms;
+  return REMD_OK;
 }
 
 remd_status remd_execute_steps_async(remd_handle h, const double* T, const double* P) {
@@ -704,8 +763,8 @@ remd_status remd_get_state(remd_handle h, int rep, remd_state_view* o) {
   o->s = st.s; o->Ps = st.Ps; o->Q = c.Q; o->W = c.W;
   for (int x = 0; x < 3; x++) { o->Pv[x] = st.Pv[x]; o->L[x] = st.L[x]; }
   o->T = st.T; o->P = st.P; o->H0 = st.H0;
-  std::vector<Part2> p2(c.ntile);
-  CK(cudaMemcpy(p2.data(), h->d.part2 + c.tile_off, c.ntile * sizeof(Part2), cudaMemcpyDeviceToHost));
+  std::vector<Part2> p2(c.nwarp);
+  CK(cudaMemcpy(p2.data(), h->d.part2 + c.warp_off, c.nwarp * sizeof(Part2), cudaMemcpyDeviceToHost));
   double lj = 0, cl = 0, w = 0, v[3] = {0, 0, 0};
   for (auto& p : p2) { lj += p.lj; cl += p.clmb; w += p.wall; for (int x = 0; x < 3; x++) v[x] += p.vir[x]; }
   o->lj = lj * 0.5; o->clmb = cl * 0.5; o->wall = w;
@@ -738,8 +797,8 @@ long long remd_replica_pair_count(remd_handle h, int rep) {
   if (!h || rep < 0 || rep >= h->nrep) return -1;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return -1;
   const RepConst& c = h->rc[rep];
-  std::vector<Part2> p2(c.ntile);
-  if (cudaMemcpy(p2.data(), h->d.part2 + c.tile_off, c.ntile * sizeof(Part2), cudaMemcpyDeviceToHost) != cudaSuccess)
+  std::vector<Part2> p2(c.nwarp);
+  if (cudaMemcpy(p2.data(), h->d.part2 + c.warp_off, c.nwarp * sizeof(Part2), cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;
   long long s = 0;
   for (auto& p : p2) s += p.npairs;

@@ -12,9 +12,10 @@
 //     tile so that the lanes of a warp read consecutive words;
 //   * per-replica scalars (thermostat, barostat, box, H0, condition) in two
 //     buffers that the integrate and force kernels ping-pong between;
-//   * per-tile partial sums written by one kernel and reduced, in a fixed
-//     order, by every CTA of the same replica in the next kernel
-//     (deterministic: a replica's result does not depend on its batch mates).
+//   * partial sums per 32 consecutive molecules of a replica (one warp),
+//     written by one kernel and reduced in molecule order by every CTA of the
+//     same replica in the next kernel (deterministic: a replica's result
+//     depends neither on its batch mates nor on the tile size).
 #pragma once
 #include <cstdint>
 
@@ -29,6 +30,7 @@ constexpr double kFixInv = 1.0 / 4294967296.0;
 struct RepConst {
   int nmol, mol_off;       // molecules; first global index
   int tile_off, ntile;     // force/integrate tiles [tile_off, tile_off+ntile)
+  int warp_off, nwarp;     // 32-molecule partial-sum units [warp_off, warp_off+nwarp)
   int nsite, c0;           // sites; first charged site (charged sites are [c0, nsite))
   int confined, tconstant, pconstant;
   int nfwall, wall_off;    // wall table entries and offset into the table array
@@ -59,7 +61,7 @@ struct RepState {
   double H0, T, P, gkT;
 };
 
-// Integrate-kernel partials of one tile.
+// Integrate-kernel partials of 32 molecules.
 struct Part1 {
   double sum_Pv[3];
   double sum_Ps;
@@ -67,7 +69,7 @@ struct Part1 {
   double pad[3];
 };
 
-// Force-kernel partials of one tile (raw ordered-pair sums; consumers halve lj/clmb/vir).
+// Force-kernel partials of 32 molecules (raw ordered-pair sums; consumers halve lj/clmb/vir).
 struct Part2 {
   double lj, clmb, wall, vir[3];
   long long npairs;        // ordered pairs within rc

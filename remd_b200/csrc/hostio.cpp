@@ -32,6 +32,7 @@ double unit_length() { return 1.0e-10; }
 double unit_energy() { return 1e3 / kNa; }
 double unit_time() { return std::sqrt(unit_mass() * unit_length() * unit_length() / unit_energy()); }
 double unit_coulomb() { return std::sqrt(4. * M_PI * kE0 * unit_energy() * unit_length()); }
+double elementary_charge() { return kEle; }
 double unit_temp() { return unit_energy() / kKB; }
 double unit_press() { return unit_energy() / (unit_length() * unit_length() * unit_length()); }
 

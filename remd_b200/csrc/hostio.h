@@ -12,6 +12,7 @@ double unit_length();
 double unit_energy();
 double unit_time();
 double unit_coulomb();
+double elementary_charge();   // C, src/unit.h
 double unit_temp();
 double unit_press();
 

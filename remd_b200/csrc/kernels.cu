@@ -48,12 +48,25 @@ __device__ inline double block_max(double v, double* sm) {
   return t;
 }
 
+// Deterministic warp reductions (fixed xor tree; lane 0's value is used).
+template <int K>
+__device__ inline void warp_sum(double* v) {
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+}
+
+__device__ inline double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 // Sum of the force partials of replica c (ordered pairs -> halved like
 // ForceCalculator::Switching, src/force_calculator.cxx:775-778).
 __device__ inline void reduce_part2(const DevPtrs& d, const RepConst& c, double& lj, double& clmb,
                                     double& wall, double* vir) {
   double a = 0, b = 0, w = 0, v0 = 0, v1 = 0, v2 = 0;
-  for (int t = c.tile_off; t < c.tile_off + c.ntile; t++) {
+  for (int t = c.warp_off; t < c.warp_off + c.nwarp; t++) {
     const Part2 p = d.part2[t];
     a += p.lj; b += p.clmb; w += p.wall;
     v0 += p.vir[0]; v1 += p.vir[1]; v2 += p.vir[2];
@@ -129,7 +142,6 @@ template <bool MID>
 __global__ void __launch_bounds__(256) k_integrate(DevPtrs d, const RepState* __restrict__ X,
                                                    RepState* __restrict__ Y, int prec) {
   __shared__ StepCoef sc;
-  __shared__ double red[8 * 5];
   const Tile t = d.tiles[blockIdx.x];
   const RepConst& c = d.rc[t.rep];
   if (threadIdx.x == 0) {
@@ -204,14 +216,15 @@ __global__ void __launch_bounds__(256) k_integrate(DevPtrs d, const RepState* __
     disp = sqrt(dx * dx + dy * dy + dz * dz);
     if (!(disp == disp)) disp = 1e30;   // NaN box: force a rebuild
   }
-  block_sum<4>(acc, red);
-  disp = block_max(disp, red);
-  if (threadIdx.x == 0) {
+  warp_sum<4>(acc);
+  disp = warp_max(disp);
+  const int w = (t.start + threadIdx.x) >> 5;   // 32-molecule unit of the replica
+  if ((threadIdx.x & 31) == 0 && w < c.nwarp) {
     Part1 pt;
     pt.sum_Pv[0] = acc[0]; pt.sum_Pv[1] = acc[1]; pt.sum_Pv[2] = acc[2];
     pt.sum_Ps = acc[3];
     pt.disp = disp;
-    d.part1[blockIdx.x] = pt;
+    d.part1[c.warp_off + w] = pt;
   }
 }
 
@@ -706,7 +719,6 @@ __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t
 template <int S, int C0, int PREC>
 __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
                            bool rebuild, int tile_size) {
-  __shared__ double red[8 * 8];
   __shared__ F32Const k32;
   extern __shared__ double acc[];   // FP32 form: (3S + 8) x blockDim.x FP64 accumulators
   const int i = threadIdx.x;
@@ -828,14 +840,15 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, i
     for (int x = 0; x < 4; x++) d.n[x * N + g] = nq[x];
   }
   double s6[7] = {a.lj, a.clmb, wall_e, a.vir[0], a.vir[1], a.vir[2], (double)a.npair};
-  block_sum<7>(s6, red);
-  if (threadIdx.x == 0) {
+  warp_sum<7>(s6);
+  const int w = (t.start + threadIdx.x) >> 5;   // 32-molecule unit of the replica
+  if ((threadIdx.x & 31) == 0 && w < c.nwarp) {
     Part2 p;
     p.lj = s6[0]; p.clmb = s6[1]; p.wall = s6[2];
     p.vir[0] = s6[3]; p.vir[1] = s6[4]; p.vir[2] = s6[5];
     p.npairs = (long long)llrint(s6[6]);
     p.pad = 0.0;
-    d.part2[tix] = p;
+    d.part2[c.warp_off + w] = p;
   }
 }
 
@@ -850,7 +863,7 @@ __global__ void __launch_bounds__(128, PREC == kF32 ? 3 : 1) k_force(DevPtrs d, 
     RepState st = Yin[t.rep];
     if (!FORCE_ONLY) {
       double sPv[3] = {0, 0, 0}, sPs = 0.0, disp = 0.0;
-      for (int k = c.tile_off; k < c.tile_off + c.ntile; k++) {
+      for (int k = c.warp_off; k < c.warp_off + c.nwarp; k++) {
         const Part1 p = d.part1[k];
         sPv[0] += p.sum_Pv[0]; sPv[1] += p.sum_Pv[1]; sPv[2] += p.sum_Pv[2];
         sPs += p.sum_Ps;
@@ -1350,7 +1363,7 @@ __global__ void k_noalloc_store(DevPtrs d, double* __restrict__ f_aos, double* _
     double lj, clmb, wall, vir[3];
     reduce_part2(d, c, lj, clmb, wall, vir);
     long long np = 0;
-    for (int t = c.tile_off; t < c.tile_off + c.ntile; t++) np += d.part2[t].npairs;
+    for (int t = c.warp_off; t < c.warp_off + c.nwarp; t++) np += d.part2[t].npairs;
     out[0] = lj; out[1] = clmb; out[2] = wall;
     out[3] = vir[0]; out[4] = vir[1]; out[5] = vir[2];
     out[6] = (double)(np / 2);

@@ -50,7 +50,7 @@ constexpr size_t kOffNbr = kOffLb + al(8 * 3 * kNoAllocMaxTiles);
 constexpr size_t kOffNbt = kOffNbr + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
 constexpr size_t kOffCnt = kOffNbt + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
 constexpr size_t kOffPart = kOffCnt + al(4 * kNoAllocMaxMol);
-constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * kNoAllocMaxTiles);
+constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * (kNoAllocMaxMol / 32));
 constexpr size_t kScratchBytes = kOffErr + al(16);
 
 // The scratch itself.  On the host this name is only a stand-in for the
@@ -144,6 +144,8 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   c.skin = kNoAllocSkin;
   c.nbr_cap = cap;
   c.ntile = (s->nmol + kNoAllocTile - 1) / kNoAllocTile;
+  c.warp_off = 0;
+  c.nwarp = (s->nmol + 31) / 32;
   c.pack_stride = pack_stride(ns, kF32);
   const double wl = s->wall_length * 1e-10 / unit_length();
   c.wall_dr = (s->confined == 2) ? 0.5 * (wl / (double)s->nfwall) : wl / (double)(s->nfwall > 0 ? s->nfwall : 1);
@@ -151,7 +153,7 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   double qr[kMaxSites];
   for (int k = 0; k < ns; k++) {
     for (int x = 0; x < 3; x++) c.body[k][x] = s->site_r[k][x] * (1e-10 / unit_length());
-    qr[k] = s->site_charge[k] * (1.6021761e-19 / unit_coulomb());
+    qr[k] = s->site_charge[k] * (elementary_charge() / unit_coulomb());
   }
   for (int k = 0; k < ns; k++)
     for (int l = 0; l < ns; l++) c.qq[k][l] = qr[k] * qr[l];

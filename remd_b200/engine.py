@@ -96,6 +96,7 @@ def lib():
         L.remd_stream.argtypes = [C.c_void_p]
         L.remd_profile_steps.argtypes = [C.c_void_p, C.c_int, _dp]
         L.remd_measure_fp32_peak.argtypes = [C.c_int, _dp]
+        L.remd_autotune.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp]
         L.remd_execute_steps_async.argtypes = [C.c_void_p, _dp, _dp]
         L.remd_get_averages.argtypes = [C.c_void_p, C.c_int, _dp]
         L.remd_get_all_averages.argtypes = [C.c_void_p, _dp]
@@ -372,6 +373,13 @@ class REMDGPU:
 
     def set_tuning(self, tile, skin):
         _check(lib().remd_set_tuning(self.h, tile, skin))
+
+    def autotune(self, nsteps=20):
+        """Pick the fastest (tile, skin) for this batch (remd_autotune); the
+        trajectory does not depend on the choice.  Returns (tile, skin, ms per step)."""
+        t, k, ms = C.c_int(), C.c_double(), C.c_double()
+        _check(lib().remd_autotune(self.h, nsteps, C.byref(t), C.byref(k), C.byref(ms)))
+        return t.value, k.value, ms.value
 
     def execute_async(self, T=None, P=None):
         if T is None:

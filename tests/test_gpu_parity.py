@@ -320,6 +320,53 @@ def test_fp32_site_image_ties_follow_oracle():
             assert np.linalg.norm(g["f"][m] - orc.f[m]) < 1e-5 * scale * 10
 
 
+def _tuning_batch():
+    return [S.small_ensemble("tip4p", 1, nmol=150, ntemp=2, npress=1, seed=81, interval=10),
+            S.small_ensemble("tip5p", 0, nmol=100, ntemp=1, npress=2, seed=82, interval=10)]
+
+
+def _run_intervals(eng, n):
+    T = np.concatenate([e.T for e in eng.ensembles])
+    P = np.concatenate([e.P for e in eng.ensembles])
+    out = []
+    for _ in range(n):
+        eng.ExecuteSteps(T, P)
+        out.append(eng.all_averages())
+    return np.array(out)
+
+
+def test_tile_and_skin_do_not_change_the_trajectory():
+    """Forces are a function of the positions only and every partial sum is per
+    32 molecules, so the same batch under different (tile, skin) choices gives
+    bit-identical averages."""
+    ens = _tuning_batch()
+    runs = []
+    for tuning in [None, (32, 0.6), (96, 1.4)]:
+        eng = E.REMDGPU(ens, precision="fp32")
+        if tuning:
+            eng.set_tuning(*tuning)
+        runs.append(_run_intervals(eng, 4))
+        eng.close()
+    assert np.array_equal(runs[0], runs[1])
+    assert np.array_equal(runs[0], runs[2])
+
+
+def test_autotune_keeps_the_trajectory():
+    """remd_autotune times its candidates on the live batch and restores the
+    state after each, so the run continues exactly as without it."""
+    ens = _tuning_batch()
+    a = E.REMDGPU(ens, precision="fp32")
+    b = E.REMDGPU(ens, precision="fp32")
+    ra, rb = [_run_intervals(a, 1)], [_run_intervals(b, 1)]
+    tile, skin, ms = a.autotune(nsteps=5)
+    assert tile in (32, 64, 96, 128) and skin in (0.6, 0.8, 1.0, 1.4) and ms > 0
+    ra.append(_run_intervals(a, 3))
+    rb.append(_run_intervals(b, 3))
+    assert np.array_equal(np.concatenate(ra), np.concatenate(rb))
+    a.close()
+    b.close()
+
+
 def test_graph_exchange_equals_explicit_exchange():
     """The exchange appended to the interval graph (device step counter, Philox
     uniforms) makes the same decisions as explicit per-interval calls."""
