@@ -65,6 +65,11 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
+    ap.add_argument("--study", choices=["drift"], default=None,
+                    help="drift: NP Hamiltonian drift of the precision-study system (config 3), "
+                         "FP32 form on every replica and FP64 vs FP32 on a subset")
+    ap.add_argument("--drift-ps", type=float, default=100.0, help="drift study length (ps)")
+    ap.add_argument("--drift-subset", type=int, default=8, help="replicas run in both forms")
     ap.add_argument("--equil-rounds", type=int, default=10,
                     help="untimed relaxation rounds of 20 steps + init_scaling")
     a = ap.parse_args(argv)
@@ -374,6 +379,88 @@ def serving_arm(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ precision study (config 3)
+def _drift_run(eng, nint, dt_ps):
+    """Advance `nint` intervals with fixed conditions (no exchange); H of every
+    replica after each interval.  Returns (t_ns, H[nint, nrep])."""
+    H = np.zeros((nint, eng.nrep))
+    for k in range(nint):
+        eng.execute_async()
+        H[k] = eng.all_averages()[:, 11]
+    t = (np.arange(nint) + 1) * dt_ps * 1e-3
+    return t, H
+
+
+def _drift_stats(t, H, nmol):
+    """Per replica: least-squares slope of H(t) in kJ/mol per ns per molecule and
+    the RMS residual about the line (kJ/mol per molecule)."""
+    A = np.stack([t, np.ones_like(t)], axis=1)
+    coef, *_ = np.linalg.lstsq(A, H, rcond=None)
+    res = H - A @ coef
+    rate = coef[0] / nmol
+    return {"rate_median_abs": float(np.median(np.abs(rate))), "rate_max_abs": float(np.max(np.abs(rate))),
+            "rate_mean": float(np.mean(rate)),
+            "residual_rms_per_mol": float(np.sqrt(np.mean(res ** 2)) / nmol),
+            "replicas": int(H.shape[1])}
+
+
+def drift_study(args, rank, world, local):
+    """NP Hamiltonian drift over `--drift-ps` of the precision-study system
+    (TIP5P N=1728 bulk, rc 12 / rs 10, 128 replicas, 3-D barostat): every replica
+    in the FP32 form, and `--drift-subset` replicas from the same equilibrated
+    start in both the FP32 and the all-FP64 form.  Conditions are fixed (no
+    exchange), so H = U + K + gkT ln s + Ps^2/2Q + Pv^2/2W + PV is conserved by
+    the Nose-Poincare/Andersen equations up to the integrator's error."""
+    import torch
+    from remd_b200 import engine as E
+    from remd_b200 import systems as S
+    from remd_b200.inputs import ReplicaState
+    if rank != 0:
+        return
+    dev = local
+    torch.cuda.set_device(dev)
+    ens = workload(3, args.seed, args.interval)
+    e0 = ens[0]
+    nmol = e0.spec.nmol
+    dt_ps = e0.spec.dt * 1e-3 * args.interval
+    nint = max(1, int(round(args.drift_ps / dt_ps)))
+    eng = E.REMDGPU(ens, precision="fp32", device=dev)
+    eng.equilibrate(rounds=args.equil_rounds, steps=20)
+    sts = []
+    for k in range(eng.nrep):
+        g = eng.ConvertVariablesToHost(k)
+        st0 = e0.states[k]
+        sts.append(ReplicaState(g["r"], g["v"], g["q"], g["p"], st0.m, st0.I, g["s"], g["Ps"], g["Q"],
+                                g["Pv"], g["W"], g["L"], g["T"], g["P"]))
+    t0 = time.perf_counter()
+    t, H32 = _drift_run(eng, nint, dt_ps)
+    wall32 = time.perf_counter() - t0
+    eng.close()
+    sub = np.linspace(0, len(sts) - 1, args.drift_subset).round().astype(int)
+    sub_states = [sts[k] for k in sub]
+    one = S.Ensemble("drift", e0.spec, len(sub), 1, np.array([s.T for s in sub_states]),
+                     np.array([s.P for s in sub_states]), sub_states)
+    out = {}
+    for prec in ("fp32", "fp64"):
+        h = E.REMDGPU([one], precision=prec, device=dev)
+        t0 = time.perf_counter()
+        _, H = _drift_run(h, nint, dt_ps)
+        out[prec] = (H, time.perf_counter() - t0)
+        h.close()
+    line = {"metric": "NP Hamiltonian drift", "unit": "kJ/mol per ns per molecule",
+            "value": _drift_stats(t, H32, nmol)["rate_median_abs"], "higher_is_better": False,
+            "study": "drift", "duration_ps": nint * dt_ps, "intervals": nint,
+            "config": {"workload": "TIP5P bulk N=1728, rc 12 / rs 10, 128 replicas, 3-D barostat, "
+                                   "fixed conditions (no exchange)", "config_index": 3,
+                       "equilibration": f"{args.equil_rounds} x (20 steps + init_scaling)"},
+            "fp32_all": dict(_drift_stats(t, H32, nmol), wall_s=wall32),
+            "subset": [int(k) for k in sub],
+            "fp32_subset": dict(_drift_stats(t, out["fp32"][0], nmol), wall_s=out["fp32"][1]),
+            "fp64_subset": dict(_drift_stats(t, out["fp64"][0], nmol), wall_s=out["fp64"][1]),
+            "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ engine arm
 def profile_traffic():
     """DRAM bytes per force launch from the committed ncu summary, if present."""
@@ -607,6 +694,8 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
+        elif args.study == "drift":
+            drift_study(args, rank, world, local)
         elif args.config == 5:
             serving_arm(args, rank, world, local)
         else:
