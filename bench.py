@@ -539,7 +539,7 @@ def engine_arm(args, rank, world, local):
     ens = rank_workload(args, rank)
     eng = E.REMDGPU(ens, precision="fp32", device=dev)
     if args.tile or args.skin:
-        eng.set_tuning(args.tile or 128, args.skin or 1.0)
+        eng.set_tuning(args.tile or 64, args.skin or 1.0)
     T = np.concatenate([e.T for e in ens])
     P = np.concatenate([e.P for e in ens])
     nmol_total = int(sum(e.spec.nmol for e in ens for _ in e.states))
@@ -551,7 +551,7 @@ def engine_arm(args, rank, world, local):
     # untimed: the autotuner picks (tile, skin) on this batch; the trajectory does
     # not depend on the choice
     if args.tile or args.skin:
-        tuning = {"tile": args.tile or 128, "skin": args.skin or 1.0, "autotuned": False}
+        tuning = {"tile": args.tile or 64, "skin": args.skin or 1.0, "autotuned": False}
     else:
         t, k, tms = eng.autotune(nsteps=20)
         tuning = {"tile": t, "skin": k, "autotuned": True, "ms_per_md_step": tms}

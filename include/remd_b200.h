@@ -191,12 +191,14 @@ remd_status remd_measure_fp32_peak(int device, double *tflops);
 /* Per-replica health word of the last interval: 0 ok, else a remd_status. */
 remd_status remd_replica_status(remd_handle h, int rep, int *status);
 
-/* Tuning: molecules of one force tile (32..128, multiple of 32) and the neighbour
+/* Tuning: molecules of one force tile (multiple of 32: 32..64 for FP32 handles,
+ * 32..128 for FP64; defaults 64 / 128) and the neighbour
  * skin (A).  Takes effect on the next call. */
 remd_status remd_set_tuning(remd_handle h, int tile, double skin);
 
 /* Autotuner (no counterpart in the reference): times every (tile, skin) of
- * {32, 64, 96, 128} x {0.6, 0.8, 1.0, 1.4} A over `nsteps` MD steps of this
+ * {32, 64, 96, 128} x {0.6, 0.8, 1.0, 1.4} A that the handle's precision
+ * allows (remd_set_tuning) over `nsteps` MD steps of this
  * batch (integrate + force per step, CUDA events), restores the state after
  * each trial and keeps the fastest.  The trajectory does not depend on the
  * choice: forces are a function of positions only and every partial sum is

@@ -166,6 +166,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       (size_t)h->nens * 8,             // 29 per-ensemble exchange seed
       (h->prec == kF32) ? (size_t)nbr_words * 2 : 0,   // 30 nbt (FP32 per-step lists)
       nt * 4,                          // 31 order
+      (h->prec == kF32) ? N * 4 : 0,   // 32 nt_cnt (FP32 per-step list counts)
   };
   offs.clear();
   total = 0;
@@ -227,6 +228,7 @@ static remd_status allocate(remd_engine_s* h) {
   h->d_seed = reinterpret_cast<unsigned long long*>(b + offs[29]);
   d.nbt = reinterpret_cast<uint16_t*>(b + offs[30]);
   d.order = reinterpret_cast<int*>(b + offs[31]);
+  d.nt_cnt = reinterpret_cast<int*>(b + offs[32]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
@@ -389,6 +391,7 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   auto* h = new remd_engine_s;
   h->device = device;
   h->prec = (prec == REMD_PREC_FP64) ? kF64 : kF32;
+  h->tile = max_force_tile(h->prec);   // 64 (FP32), 128 (FP64); remd_set_tuning / remd_autotune change it
   h->nens = nens;
   h->interval = systems[0].interval;
   h->sys.assign(systems, systems + nens);
@@ -628,8 +631,8 @@ static remd_status relayout(remd_engine_s* h, int tile, double skin, const Saved
 }
 
 remd_status remd_set_tuning(remd_handle h, int tile, double skin) {
-  if (!h || tile < 32 || tile > 128 || tile % 32 || !(skin > 0.0)) {
-    set_error("remd_set_tuning: tile must be 32..128 (multiple of 32), skin > 0");
+  if (!h || tile < 32 || tile > max_force_tile(h->prec) || tile % 32 || !(skin > 0.0)) {
+    set_error("remd_set_tuning: tile must be a multiple of 32 in 32..64 (FP32) or 32..128 (FP64), skin > 0");
     return REMD_ERR_INVALID;
   }
   if (tile == h->tile && skin == h->skin) return REMD_OK;
@@ -650,6 +653,7 @@ remd_status remd_autotune(remd_handle h, int nsteps, int* tile_out, double* skin
   double best_skin = h->skin, best_ms = 1e300;
   for (int t : tiles)
     for (double k : skins) {
+      if (t > max_force_tile(h->prec)) continue;
       if ((s = relayout(h, t, k, sv)) != REMD_OK) return s;
       double ms[2];
       if ((s = remd_profile_steps(h, nsteps, ms)) != REMD_OK) return s;
@@ -791,7 +795,12 @@ long long remd_last_pair_count(remd_handle h) {
   h->last_pairs = host_pairs(h);
   return h->last_pairs;
 }
-int remd_launches_per_interval(remd_handle h) { return h ? 2 * h->interval + 2 : 0; }
+int remd_launches_per_interval(remd_handle h) {
+  // replica_start + per MD step (integrate, force: lists + pairs in FP32, one launch in FP64)
+  // + replica_end + the device exchange when enabled
+  if (!h) return 0;
+  return (h->prec == kF32 ? 3 : 2) * h->interval + 2 + (h->exch_enabled ? 1 : 0);
+}
 
 long long remd_replica_pair_count(remd_handle h, int rep) {
   if (!h || rep < 0 || rep >= h->nrep) return -1;

@@ -93,6 +93,7 @@ struct DevPtrs {
   double* Lbuild;                // per tile, 3 doubles (NaN = list invalid)
   uint16_t* nbr;                 // neighbour lists (rcut + skin)
   uint16_t* nbt;                 // FP32 form: per-step lists of the pairs within rcut (same layout)
+  int* nt_cnt;                   // FP32 form: per molecule, nfar | nnear << 16 in nbt
   int* nbr_cnt;                  // per molecule
   const double* wall;            // {f, U} pairs
   Part1* part1;

@@ -319,15 +319,17 @@ struct IAcc {
   long long npair;
 };
 
-// FP32 pair loop over i's neighbour list, in two passes.
-// Pass 1 scans the (rcut + skin) list and writes the neighbours within rcut, in
-// the list's ascending-j order, to i's column of the per-step list `nbt` (same
-// layout and capacity as the skin list; it cannot overflow).  Under the
+// FP32 pair loop over i's neighbour list, in two passes run by two kernels.
+// Pass 1 (k_force_lists) scans the (rcut + skin) list and writes the neighbours
+// within rcut, in the list's ascending-j order, to i's column of the per-step
+// list `nbt` (same layout and capacity as the skin list; it cannot overflow).  Under the
 // per-site minimum image (SIMG, below) it splits them: pairs whose COM vector
 // keeps every site-pair component clear of +-L/2 ("far", from the front of the
 // column) need no per-site image at all; the others ("near", from the back)
 // get the per-site image.  Pass 2 computes exactly those pairs, so the lanes of
-// a warp stay converged (no cutoff branch) and differ only in their counts.
+// a warp stay converged (no cutoff branch) and differ only in their counts
+// (k_force_pairs).  Pass 1 runs in its own light kernel, whose occupancy hides
+// the latency of its gathered loads; pass 2 is register-heavy.
 // Pair math in FP32 (rsqrt on the SFU plus one Newton step); partial sums in
 // FP32 over 16 pairs, then FP64 accumulation into this thread's slots of `acc`
 // (shared memory, field f at acc[f * blockDim.x + threadIdx.x]: 3S site-force
@@ -426,16 +428,72 @@ __device__ __noinline__ void site_pair_exact(const DevPtrs& d, const RepConst& c
   acc[(3 * S + 7) * T + tid] += (double)(sw * ecl);
 }
 
+// Pass 1 for molecule li of tile t: the neighbours of its (rcut + skin) list
+// that are within rcut, in ascending j, into its column of `nt` -- far pairs
+// from the front, near pairs (SIMG only) from the back -- eight candidates per
+// round so that their record loads are in flight together.  Stores
+// nfar | nnear << 16 in d.nt_cnt.
+template <bool SIMG>
+__device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, const double* L,
+                                const uint16_t* nb, uint16_t* nt, int cnt) {
+  const int T = blockDim.x;
+  const int nv = c.pack_stride / 4;   // uint4 per record
+  const uint4* base = reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off);
+  const float Ls0 = (float)(L[0] * kFixInv), Ls1 = (float)(L[1] * kFixInv), Ls2 = (float)(L[2] * kFixInv);
+  const float rc2 = (float)(c.rc * c.rc);
+  const uint4 ui = __ldg(base + (long long)li * nv);
+  const int xi = (int)ui.x, yi = (int)ui.y, zi = (int)ui.z;
+  // far bound: |d_x| below it keeps every site-pair component below L/2 - kImageTol
+  float bnd0 = 0.f, bnd1 = 0.f, bnd2 = 0.f;
+  if (SIMG) {
+    const float m = 2.f * (float)c.site_reach + kImageTol + 1e-3f;
+    bnd0 = 0.5f * (float)L[0] - m; bnd1 = 0.5f * (float)L[1] - m; bnd2 = 0.5f * (float)L[2] - m;
+  }
+  const int back = c.nbr_cap - 1;
+  int nfar = 0, nnear = 0;
+  auto keep = [&](int j, float dx, float dy, float dz) {
+    if (dx * dx + dy * dy + dz * dz <= rc2) {
+      if (SIMG && (fabsf(dx) >= bnd0 || fabsf(dy) >= bnd1 || fabsf(dz) >= bnd2)) {
+        nt[(long long)(back - nnear) * T] = (uint16_t)j;
+        nnear++;
+      } else {
+        nt[(long long)nfar * T] = (uint16_t)j;
+        nfar++;
+      }
+    }
+  };
+  constexpr int B = 8;
+  int k = 0;
+  for (; k + B <= cnt; k += B) {
+    int j[B];
+    uint4 u[B];
+#pragma unroll
+    for (int m = 0; m < B; m++) j[m] = nb[(long long)(k + m) * T];
+#pragma unroll
+    for (int m = 0; m < B; m++) u[m] = __ldg(base + (long long)j[m] * nv);
+#pragma unroll
+    for (int m = 0; m < B; m++)
+      keep(j[m], (float)(int)(xi - (int)u[m].x) * Ls0, (float)(int)(yi - (int)u[m].y) * Ls1,
+           (float)(int)(zi - (int)u[m].z) * Ls2);
+  }
+  for (; k < cnt; k++) {
+    const int j = nb[(long long)k * T];
+    const uint4 u = __ldg(base + (long long)j * nv);
+    keep(j, (float)(int)(xi - (int)u.x) * Ls0, (float)(int)(yi - (int)u.y) * Ls1,
+         (float)(int)(zi - (int)u.z) * Ls2);
+  }
+  d.nt_cnt[c.mol_off + li] = nfar | (nnear << 16);
+}
+
 template <int S, int C0, bool SIMG>
-__device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const F32Const& k32,
-                              const uint16_t* nb, uint16_t* nt, int cnt, double* acc, long long& npair) {
+__device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const F32Const& k32, int li,
+                              const uint16_t* nt, int lstride, int nfar, int nnear, int p0, int p1,
+                              double* acc) {
   constexpr int STRIDE = ((3 + 3 * S) + 3) / 4 * 4;
   constexpr int NV = STRIDE / 4;
-  const int T = blockDim.x, tid = threadIdx.x;
-  const int li = t.start + tid;
+  const int T = blockDim.x, tid = threadIdx.x;   // accumulator slots
   const uint4* base = reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off);
   const float Ls0 = k32.Ls[0], Ls1 = k32.Ls[1], Ls2 = k32.Ls[2];
-  const float rc2 = (float)(c.rc * c.rc);
   int xi, yi, zi;
   float si[S][3];
   {
@@ -451,49 +509,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
 #pragma unroll
       for (int x = 0; x < 3; x++) si[k][x] = __uint_as_float(wi[3 + 3 * k + x]);
   }
-  // far bound: |d_x| below it keeps every site-pair component below L/2 - kImageTol
-  float bnd0 = 0.f, bnd1 = 0.f, bnd2 = 0.f;
-  if (SIMG) {
-    const float m = 2.f * (float)c.site_reach + kImageTol + 1e-3f;
-    bnd0 = k32.hL[0] - m; bnd1 = k32.hL[1] - m; bnd2 = k32.hL[2] - m;
-  }
   const int back = c.nbr_cap - 1;
-  // pass 1: neighbours within rcut (same FP32 distance as pass 2), eight
-  // candidates per round so that their loads are in flight together
-  int nfar = 0, nnear = 0;
-  auto keep = [&](int j, float dx, float dy, float dz) {
-    if (dx * dx + dy * dy + dz * dz <= rc2) {
-      if (SIMG && (fabsf(dx) >= bnd0 || fabsf(dy) >= bnd1 || fabsf(dz) >= bnd2)) {
-        nt[(long long)(back - nnear) * T] = (uint16_t)j;
-        nnear++;
-      } else {
-        nt[(long long)nfar * T] = (uint16_t)j;
-        nfar++;
-      }
-    }
-  };
-  {
-    constexpr int B = 8;
-    int k = 0;
-    for (; k + B <= cnt; k += B) {
-      int j[B];
-      uint4 u[B];
-#pragma unroll
-      for (int m = 0; m < B; m++) j[m] = nb[(long long)(k + m) * T];
-#pragma unroll
-      for (int m = 0; m < B; m++) u[m] = __ldg(base + (long long)j[m] * NV);
-#pragma unroll
-      for (int m = 0; m < B; m++)
-        keep(j[m], (float)(int)(xi - (int)u[m].x) * Ls0, (float)(int)(yi - (int)u[m].y) * Ls1,
-             (float)(int)(zi - (int)u[m].z) * Ls2);
-    }
-    for (; k < cnt; k++) {
-      const int j = nb[(long long)k * T];
-      const uint4 u = __ldg(base + (long long)j * NV);
-      keep(j, (float)(int)(xi - (int)u.x) * Ls0, (float)(int)(yi - (int)u.y) * Ls1,
-           (float)(int)(zi - (int)u.z) * Ls2);
-    }
-  }
   const float rc = (float)c.rc, rs = (float)c.rs;
   const float coef = (float)c.coef_sw;
   const float sgm2 = (float)c.sgm2, eps4 = (float)(4.0 * c.eps), eps48 = (float)(48.0 * c.eps);
@@ -530,10 +546,10 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
     const float hL0 = k32.hL[0], hL1 = k32.hL[1], hL2 = k32.hL[2];
     const float Lf0 = k32.Lf[0], Lf1 = k32.Lf[1], Lf2 = k32.Lf[2];
     uint4 nx[NV];
-    int jnext = (n > 1) ? nt[(long long)(pos0 + dir) * T] : 0;
+    int jnext = (n > 1) ? nt[(long long)(pos0 + dir) * lstride] : 0;
     int jpre = 0;
     if (n > 0) {
-      const int j0 = nt[(long long)pos0 * T];
+      const int j0 = nt[(long long)pos0 * lstride];
       jpre = j0;
 #pragma unroll
       for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)j0 * NV + m);
@@ -548,7 +564,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
       if (k + 1 < n) {
         const int jn = jnext;
         jpre = jn;
-        if (k + 2 < n) jnext = nt[(long long)(pos0 + dir * (k + 2)) * T];
+        if (k + 2 < n) jnext = nt[(long long)(pos0 + dir * (k + 2)) * lstride];
 #pragma unroll
         for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
       }
@@ -628,14 +644,18 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const Tile& t
       if ((++done & 15) == 0) { flush(); zero(); }
     }
   };
-  run(std::false_type{}, nfar, 0, 1);
-  if (SIMG) run(std::true_type{}, nnear, back, -1);
+  // positions [p0, p1) of the sequence far pairs (rows 0..) then near pairs (rows back, back-1, ..)
+  const int f1 = min(p1, nfar);
+  run(std::false_type{}, max(f1 - p0, 0), p0, 1);
+  if (SIMG) {
+    const int q0 = max(p0, nfar);
+    run(std::true_type{}, max(p1 - q0, 0), back - (q0 - nfar), -1);
+  }
   flush();
   if (SIMG && ndef > 0) {
     site_pair_exact<S, C0>(d, c, k32, li, def0, acc);
     if (ndef > 1) site_pair_exact<S, C0>(d, c, k32, li, def1, acc);
   }
-  npair += nfar + nnear;
 }
 
 template <int S, int C0, bool SIMG>
@@ -716,129 +736,65 @@ __device__ void pair_loop_f64(const DevPtrs& d, const RepConst& c, const Tile& t
   }
 }
 
-template <int S, int C0, int PREC>
-__device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
-                           bool rebuild, int tile_size) {
-  __shared__ F32Const k32;
-  extern __shared__ double acc[];   // FP32 form: (3S + 8) x blockDim.x FP64 accumulators
-  const int i = threadIdx.x;
-  const bool valid = i < t.count;
-  const int li = t.start + i;
-  const int g = c.mol_off + li;
-  const int T = blockDim.x;
-  uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
-  if (rebuild) {
-    build_lists<PREC>(d, c, t, L, nb, tile_size);
-    __syncthreads();
-    if (valid) {
-      const int* w;
-      int4 rc4;
-      if (PREC == kF32) {
-        w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-        rc4 = make_int4(w[0], w[1], w[2], 0);
-      } else {
-        const double* wd = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-        rc4 = make_int4(fix_coord(wd[0]), fix_coord(wd[1]), fix_coord(wd[2]), 0);
-      }
-      d.ref_com[g] = rc4;
-    }
-    if (i == 0)
-      for (int x = 0; x < 3; x++) d.Lbuild[3 * tix + x] = L[x];
-  }
-  if (PREC == kF32) {
-    if (i == 0) {
-      for (int k = 0; k < kMaxSites; k++)
-        for (int l = 0; l < kMaxSites; l++) k32.qq[k][l] = (float)c.qq[k][l];
-      for (int x = 0; x < 3; x++) {
-        k32.Ls[x] = (float)(L[x] * kFixInv);
-        k32.Lf[x] = (float)L[x];
-        k32.hL[x] = 0.5f * (float)L[x];
-        k32.L[x] = L[x];
-      }
-    }
-    for (int f = 0; f < 3 * S + 8; f++) acc[f * T + i] = 0.0;
-    __syncthreads();
-  }
-  IAcc a;
-#pragma unroll
-  for (int k = 0; k < kMaxSites; k++) a.fs[k][0] = a.fs[k][1] = a.fs[k][2] = 0.0;
-  a.fc[0] = a.fc[1] = a.fc[2] = 0.0;
-  a.vir[0] = a.vir[1] = a.vir[2] = 0.0;
-  a.lj = a.clmb = 0.0;
-  a.npair = 0;
-  double wall_e = 0.0;
-  if (valid) {
-    const int cnt = d.nbr_cnt[g];
-    const double reach = c.rc + 2.0 * c.site_reach;
-    const bool simg = (L[0] < 2.0 * reach) || (L[1] < 2.0 * reach) || (L[2] < 2.0 * reach);
-    if (PREC == kF32) {
-      uint16_t* nt = d.nbt + (nb - d.nbr);
-      if (simg) pair_loop_f32<S, C0, true>(d, c, t, k32, nb, nt, cnt, acc, a.npair);
-      else pair_loop_f32<S, C0, false>(d, c, t, k32, nb, nt, cnt, acc, a.npair);
-#pragma unroll
-      for (int k = 0; k < S; k++)
-        for (int x = 0; x < 3; x++) a.fs[k][x] = acc[(3 * k + x) * T + i];
-      for (int x = 0; x < 3; x++) {
-        a.fc[x] = acc[(3 * S + x) * T + i];
-        a.vir[x] = acc[(3 * S + 3 + x) * T + i];
-      }
-      a.lj = acc[(3 * S + 6) * T + i];
-      a.clmb = acc[(3 * S + 7) * T + i];
+// Wall on the oxygen site and A2M for molecule g (FP64): writes d.f, d.n.
+template <int S>
+__device__ void finish_molecule(const DevPtrs& d, const RepConst& c, int g, const double* L, IAcc& a,
+                                double& wall_e) {
+  const int N = d.N;
+  double q[4], r[3];
+  for (int x = 0; x < 4; x++) q[x] = d.q[x * N + g];
+  for (int x = 0; x < 3; x++) r[x] = d.r[x * N + g];
+  // wall on the oxygen site (ForceCalculator::Confined, src/force_calculator.cxx:1527-1566;
+  // slit: src/remdgpu.cu:1708-1720)
+  if (c.confined > 0) {
+    double o[3];
+    body_to_space(q, c.body[0], o);
+    const double2* fw = reinterpret_cast<const double2*>(d.wall) + c.wall_off;
+    const double dr = c.wall_dr;
+    if (c.confined == 1) {
+      const double x = r[0] * L[0] + o[0] - L[0] * 0.5;
+      const double y = r[1] * L[1] + o[1] - L[1] * 0.5;
+      const double r01 = sqrt(x * x + y * y);
+      int idx = (r01 >= 0.0) ? (int)fmin(r01 / dr, (double)(c.nfwall - 2)) : 0;   // NaN -> 0
+      const double2 w0 = fw[idx], w1 = fw[idx + 1];
+      const double f = (w1.x - w0.x) / dr * (r01 - dr * idx) + w0.x;
+      const double e = (w1.y - w0.y) / dr * (r01 - dr * idx) + w0.y;
+      a.fs[0][0] += f * x;
+      a.fs[0][1] += f * y;
+      wall_e = e;
     } else {
-      if (simg) pair_loop_f64<S, C0, true>(d, c, t, L, nb, cnt, a);
-      else pair_loop_f64<S, C0, false>(d, c, t, L, nb, cnt, a);
+      const double z = r[2] * L[2] + o[2] - 0.5 * L[2];
+      const double za = fabs(z);
+      const double dir = (za != 0.0) ? z / za : 1.0;
+      int idx = (za >= 0.0) ? (int)fmin(za / dr, (double)(c.nfwall - 2)) : 0;     // NaN -> 0
+      const double2 w0 = fw[idx], w1 = fw[idx + 1];
+      const double f = (w1.x - w0.x) / dr * (za - dr * idx) + w0.x;
+      const double e = (w1.y - w0.y) / dr * (za - dr * idx) + w0.y;
+      a.fs[0][2] += f * dir;
+      wall_e = e;
     }
-    const int N = d.N;
-    double q[4], r[3];
-    for (int x = 0; x < 4; x++) q[x] = d.q[x * N + g];
-    for (int x = 0; x < 3; x++) r[x] = d.r[x * N + g];
-    // wall on the oxygen site (ForceCalculator::Confined, src/force_calculator.cxx:1527-1566;
-    // slit: src/remdgpu.cu:1708-1720)
-    if (c.confined > 0) {
-      double o[3];
-      body_to_space(q, c.body[0], o);
-      const double2* fw = reinterpret_cast<const double2*>(d.wall) + c.wall_off;
-      const double dr = c.wall_dr;
-      if (c.confined == 1) {
-        const double x = r[0] * L[0] + o[0] - L[0] * 0.5;
-        const double y = r[1] * L[1] + o[1] - L[1] * 0.5;
-        const double r01 = sqrt(x * x + y * y);
-        int idx = (r01 >= 0.0) ? (int)fmin(r01 / dr, (double)(c.nfwall - 2)) : 0;   // NaN -> 0
-        const double2 w0 = fw[idx], w1 = fw[idx + 1];
-        const double f = (w1.x - w0.x) / dr * (r01 - dr * idx) + w0.x;
-        const double e = (w1.y - w0.y) / dr * (r01 - dr * idx) + w0.y;
-        a.fs[0][0] += f * x;
-        a.fs[0][1] += f * y;
-        wall_e = e;
-      } else {
-        const double z = r[2] * L[2] + o[2] - 0.5 * L[2];
-        const double za = fabs(z);
-        const double dir = (za != 0.0) ? z / za : 1.0;
-        int idx = (za >= 0.0) ? (int)fmin(za / dr, (double)(c.nfwall - 2)) : 0;     // NaN -> 0
-        const double2 w0 = fw[idx], w1 = fw[idx + 1];
-        const double f = (w1.x - w0.x) / dr * (za - dr * idx) + w0.x;
-        const double e = (w1.y - w0.y) / dr * (za - dr * idx) + w0.y;
-        a.fs[0][2] += f * dir;
-        wall_e = e;
-      }
-    }
-    // A2M: molecular force and body torque (src/molecules.cxx:447-475)
-    double F[3] = {a.fc[0], a.fc[1], a.fc[2]};
-    double nq[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-      for (int x = 0; x < 3; x++) F[x] += a.fs[k][x];
-      double fb[3];
-      space_to_body(q, a.fs[k], fb);
-      const double* b = c.body[k];
-      nq[0] += b[0] * fb[0] + b[1] * fb[1] + b[2] * fb[2];
-      nq[1] += b[1] * fb[2] - b[2] * fb[1];
-      nq[2] += b[2] * fb[0] - b[0] * fb[2];
-      nq[3] += b[0] * fb[1] - b[1] * fb[0];
-    }
-    for (int x = 0; x < 3; x++) d.f[x * N + g] = F[x];
-    for (int x = 0; x < 4; x++) d.n[x * N + g] = nq[x];
   }
+  // A2M: molecular force and body torque (src/molecules.cxx:447-475)
+  double F[3] = {a.fc[0], a.fc[1], a.fc[2]};
+  double nq[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < S; k++) {
+    for (int x = 0; x < 3; x++) F[x] += a.fs[k][x];
+    double fb[3];
+    space_to_body(q, a.fs[k], fb);
+    const double* b = c.body[k];
+    nq[0] += b[0] * fb[0] + b[1] * fb[1] + b[2] * fb[2];
+    nq[1] += b[1] * fb[2] - b[2] * fb[1];
+    nq[2] += b[2] * fb[0] - b[0] * fb[2];
+    nq[3] += b[0] * fb[1] - b[1] * fb[0];
+  }
+  for (int x = 0; x < 3; x++) d.f[x * N + g] = F[x];
+  for (int x = 0; x < 4; x++) d.n[x * N + g] = nq[x];
+}
+
+// Force partials of the tile's 32-molecule units (one fixed shuffle tree per warp).
+__device__ inline void write_part2(const DevPtrs& d, const RepConst& c, const Tile& t, const IAcc& a,
+                                   double wall_e) {
   double s6[7] = {a.lj, a.clmb, wall_e, a.vir[0], a.vir[1], a.vir[2], (double)a.npair};
   warp_sum<7>(s6);
   const int w = (t.start + threadIdx.x) >> 5;   // 32-molecule unit of the replica
@@ -852,49 +808,225 @@ __device__ void force_tile(const DevPtrs& d, const RepConst& c, const Tile& t, i
   }
 }
 
-template <int PREC, bool FORCE_ONLY>
-__global__ void __launch_bounds__(128, PREC == kF32 ? 3 : 1) k_force(DevPtrs d, const RepState* __restrict__ Yin,
-                                               RepState* __restrict__ Xout, int tile_size) {
+__device__ inline void zero_acc(IAcc& a) {
+#pragma unroll
+  for (int k = 0; k < kMaxSites; k++) a.fs[k][0] = a.fs[k][1] = a.fs[k][2] = 0.0;
+  a.fc[0] = a.fc[1] = a.fc[2] = 0.0;
+  a.vir[0] = a.vir[1] = a.vir[2] = 0.0;
+  a.lj = a.clmb = 0.0;
+  a.npair = 0;
+}
+
+// Skin-list rebuild of tile t when due, with the build's reference centres and box.
+template <int PREC>
+__device__ void rebuild_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
+                             uint16_t* nb, int tile_size) {
+  const int i = threadIdx.x;
+  const int li = t.start + i;
+  build_lists<PREC>(d, c, t, L, nb, tile_size);
+  __syncthreads();
+  if (i < t.count) {
+    int4 rc4;
+    if (PREC == kF32) {
+      const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+      rc4 = make_int4(w[0], w[1], w[2], 0);
+    } else {
+      const double* wd = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+      rc4 = make_int4(fix_coord(wd[0]), fix_coord(wd[1]), fix_coord(wd[2]), 0);
+    }
+    d.ref_com[c.mol_off + li] = rc4;
+  }
+  if (i == 0)
+    for (int x = 0; x < 3; x++) d.Lbuild[3 * tix + x] = L[x];
+}
+
+__device__ inline bool site_image_needed(const RepConst& c, const double* L) {
+  const double reach = c.rc + 2.0 * c.site_reach;
+  return (L[0] < 2.0 * reach) || (L[1] < 2.0 * reach) || (L[2] < 2.0 * reach);
+}
+
+// FP64 form: rebuild when due, pair loop, wall, A2M.
+template <int S, int C0>
+__device__ void force_tile_f64(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
+                               bool rebuild, int tile_size) {
+  const int i = threadIdx.x;
+  const int li = t.start + i;
+  const int g = c.mol_off + li;
+  uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
+  if (rebuild) rebuild_tile<kF64>(d, c, t, tix, L, nb, tile_size);
+  IAcc a;
+  zero_acc(a);
+  double wall_e = 0.0;
+  if (i < t.count) {
+    const int cnt = d.nbr_cnt[g];
+    if (site_image_needed(c, L)) pair_loop_f64<S, C0, true>(d, c, t, L, nb, cnt, a);
+    else pair_loop_f64<S, C0, false>(d, c, t, L, nb, cnt, a);
+    finish_molecule<S>(d, c, g, L, a, wall_e);
+  }
+  write_part2(d, c, t, a, wall_e);
+}
+
+// FP32 form, pass 2 + wall + A2M (the per-step list comes from k_force_lists).
+// Two threads per molecule: thread (i, ch) computes positions [ch n/2, (ch+1) n/2)
+// of i's n pairs, so a launch has twice the work units (a shorter tail); the
+// two FP64 partials are added in chunk order.  The split is by list position
+// and the list holds exactly the pairs within rcut in ascending j, so results
+// depend neither on the tile size nor on the list history.
+constexpr int kPairChunks = 2;
+
+template <int S, int C0>
+__device__ void force_tile_f32(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
+                               int tile_size) {
+  __shared__ F32Const k32;
+  extern __shared__ double acc[];   // (3S + 8) x blockDim.x FP64 accumulators
+  const int B = blockDim.x;
+  const int i = threadIdx.x % tile_size, ch = threadIdx.x / tile_size;
+  const int li = t.start + i;
+  const int g = c.mol_off + li;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kMaxSites; k++)
+      for (int l = 0; l < kMaxSites; l++) k32.qq[k][l] = (float)c.qq[k][l];
+    for (int x = 0; x < 3; x++) {
+      k32.Ls[x] = (float)(L[x] * kFixInv);
+      k32.Lf[x] = (float)L[x];
+      k32.hL[x] = 0.5f * (float)L[x];
+      k32.L[x] = L[x];
+    }
+  }
+  for (int f = 0; f < 3 * S + 8; f++) acc[f * B + threadIdx.x] = 0.0;
+  __syncthreads();
+  int npairs = 0;
+  if (i < t.count) {
+    const uint16_t* nt = d.nbt + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
+    const int nc = d.nt_cnt[g];
+    const int nfar = nc & 0xffff, nnear = nc >> 16;
+    npairs = nfar + nnear;
+    const int p0 = (npairs * ch) / kPairChunks, p1 = (npairs * (ch + 1)) / kPairChunks;
+    if (site_image_needed(c, L))
+      pair_loop_f32<S, C0, true>(d, c, k32, li, nt, tile_size, nfar, nnear, p0, p1, acc);
+    else
+      pair_loop_f32<S, C0, false>(d, c, k32, li, nt, tile_size, nfar, nnear, p0, p1, acc);
+  }
+  __syncthreads();
+  if (ch != 0) return;   // chunk-0 threads (whole warps) finish the molecules
+  IAcc a;
+  zero_acc(a);
+  double wall_e = 0.0;
+  if (i < t.count) {
+    auto sum = [&](int f) {
+      double v = 0.0;
+      for (int k = 0; k < kPairChunks; k++) v += acc[f * B + i + k * tile_size];
+      return v;
+    };
+#pragma unroll
+    for (int k = 0; k < S; k++)
+      for (int x = 0; x < 3; x++) a.fs[k][x] = sum(3 * k + x);
+    for (int x = 0; x < 3; x++) {
+      a.fc[x] = sum(3 * S + x);
+      a.vir[x] = sum(3 * S + 3 + x);
+    }
+    a.lj = sum(3 * S + 6);
+    a.clmb = sum(3 * S + 7);
+    a.npair = npairs;
+    finish_molecule<S>(d, c, g, L, a, wall_e);
+  }
+  write_part2(d, c, t, a, wall_e);
+}
+
+// Head of a force step (thread 0): PsPv and D4 with the integrate kernel's
+// partials (src/integrator.cxx:132-172, 604-632), the replica's new scalars to
+// Xout (first tile), and whether this tile's skin list must be rebuilt.
+template <bool FORCE_ONLY>
+__device__ void force_head(const DevPtrs& d, const RepConst& c, int rep, int tix, const RepState* Yin,
+                           RepState* Xout, ForceHead& h) {
+  RepState st = Yin[rep];
+  if (!FORCE_ONLY) {
+    double sPv[3] = {0, 0, 0}, sPs = 0.0, disp = 0.0;
+    for (int k = c.warp_off; k < c.warp_off + c.nwarp; k++) {
+      const Part1 p = d.part1[k];
+      sPv[0] += p.sum_Pv[0]; sPv[1] += p.sum_Pv[1]; sPv[2] += p.sum_Pv[2];
+      sPs += p.sum_Ps;
+      disp = fmax(disp, p.disp);
+    }
+    pspv(c, st, sPv, sPs);
+    d4(c, st);
+    if (tix == c.tile_off) Xout[rep] = st;
+    // list validity: pairs now within rc were within rc+skin at the build if
+    // 2*max|displacement| + rc*(max_d Lbuild_d/L_d - 1) <= skin
+    const double lb0 = d.Lbuild[3 * tix], lb1 = d.Lbuild[3 * tix + 1], lb2 = d.Lbuild[3 * tix + 2];
+    int rb = !(lb0 == lb0);
+    if (!rb) {
+      const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
+      rb = (2.0 * disp + c.rc * (lam - 1.0) > c.skin);
+    }
+    h.rebuild = rb;
+  } else {
+    h.rebuild = 1;
+  }
+  for (int x = 0; x < 3; x++) h.L[x] = st.L[x];
+}
+
+// FP64 form: one launch per step (head, rebuild, pairs, wall, A2M).
+template <bool FORCE_ONLY>
+__global__ void __launch_bounds__(128) k_force_f64(DevPtrs d, const RepState* __restrict__ Yin,
+                                                   RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
   const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;   // costliest tiles first
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
-  if (threadIdx.x == 0) {
-    RepState st = Yin[t.rep];
-    if (!FORCE_ONLY) {
-      double sPv[3] = {0, 0, 0}, sPs = 0.0, disp = 0.0;
-      for (int k = c.warp_off; k < c.warp_off + c.nwarp; k++) {
-        const Part1 p = d.part1[k];
-        sPv[0] += p.sum_Pv[0]; sPv[1] += p.sum_Pv[1]; sPv[2] += p.sum_Pv[2];
-        sPs += p.sum_Ps;
-        disp = fmax(disp, p.disp);
-      }
-      pspv(c, st, sPv, sPs);
-      d4(c, st);
-      if (tix == c.tile_off) Xout[t.rep] = st;
-      // list validity: pairs now within rc were within rc+skin at the build if
-      // 2*max|displacement| + rc*(max_d Lbuild_d/L_d - 1) <= skin
-      const double lb0 = d.Lbuild[3 * tix], lb1 = d.Lbuild[3 * tix + 1], lb2 = d.Lbuild[3 * tix + 2];
-      int rb = !(lb0 == lb0);
-      if (!rb) {
-        const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
-        rb = (2.0 * disp + c.rc * (lam - 1.0) > c.skin);
-      }
-      h.rebuild = rb;
-    } else {
-      h.rebuild = 1;
-    }
-    for (int x = 0; x < 3; x++) h.L[x] = st.L[x];
-  }
+  if (threadIdx.x == 0) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
   __syncthreads();
   const double L[3] = {h.L[0], h.L[1], h.L[2]};
   const bool rb = h.rebuild != 0;
   if (c.nsite == 3)
-    force_tile<3, 0, PREC>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<3, 0>(d, c, t, tix, L, rb, tile_size);
   else if (c.nsite == 4)
-    force_tile<4, 1, PREC>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<4, 1>(d, c, t, tix, L, rb, tile_size);
   else
-    force_tile<5, 1, PREC>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<5, 1>(d, c, t, tix, L, rb, tile_size);
+}
+
+// FP32 form, first launch of a step: head, skin-list rebuild when due, pass 1.
+// Light on registers, so many warps hide the gathered loads of pass 1.
+template <bool FORCE_ONLY>
+__global__ void __launch_bounds__(128, 8) k_force_lists(DevPtrs d, const RepState* __restrict__ Yin,
+                                                     RepState* __restrict__ Xout, int tile_size) {
+  __shared__ ForceHead h;
+  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;
+  const Tile t = d.tiles[tix];
+  const RepConst& c = d.rc[t.rep];
+  if (threadIdx.x == 0) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
+  __syncthreads();
+  const double L[3] = {h.L[0], h.L[1], h.L[2]};
+  const int i = threadIdx.x;
+  const int li = t.start + i;
+  uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
+  if (h.rebuild) rebuild_tile<kF32>(d, c, t, tix, L, nb, tile_size);
+  if (i < t.count) {
+    uint16_t* nt = d.nbt + (nb - d.nbr);
+    const int cnt = d.nbr_cnt[c.mol_off + li];
+    if (site_image_needed(c, L)) tight_lists_f32<true>(d, c, li, L, nb, nt, cnt);
+    else tight_lists_f32<false>(d, c, li, L, nb, nt, cnt);
+  }
+}
+
+// FP32 form, second launch of a step: pair forces, wall, A2M (box from X, which
+// k_force_lists has updated); kPairChunks x tile threads.
+__global__ void __launch_bounds__(128, 3) k_force_pairs(DevPtrs d, const RepState* __restrict__ X,
+                                                        int tile_size) {
+  __shared__ double Ls[3];
+  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;
+  const Tile t = d.tiles[tix];
+  const RepConst& c = d.rc[t.rep];
+  if (threadIdx.x < 3) Ls[threadIdx.x] = X[t.rep].L[threadIdx.x];
+  __syncthreads();
+  const double L[3] = {Ls[0], Ls[1], Ls[2]};
+  if (c.nsite == 3)
+    force_tile_f32<3, 0>(d, c, t, tix, L, tile_size);
+  else if (c.nsite == 4)
+    force_tile_f32<4, 1>(d, c, t, tix, L, tile_size);
+  else
+    force_tile_f32<5, 1>(d, c, t, tix, L, tile_size);
 }
 
 // ------------------------------------------------------------------ per-replica kernels
@@ -1390,6 +1522,8 @@ void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, boo
   else
     k_integrate<false><<<d.ntiles, tile, 0, s>>>(d, X, Y, prec);
 }
+int max_force_tile(int prec) { return prec == kF32 ? 128 / kPairChunks : 128; }
+
 size_t force_smem_bytes(int tile) { return (size_t)(3 * kMaxSites + 8) * tile * sizeof(double); }
 
 cudaError_t force_kernel_setup() {
@@ -1397,21 +1531,18 @@ cudaError_t force_kernel_setup() {
   // of up to 128 molecules (23.5 KB, under the default limit; set explicitly so
   // that a larger tile or more accumulators only change force_smem_bytes)
   const int sm = (int)force_smem_bytes(128);
-  cudaError_t e = cudaFuncSetAttribute(k_force<kF32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_force<kF32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  return e;
+  return cudaFuncSetAttribute(k_force_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s) {
   if (prec == kF32) {
-    const size_t sm = force_smem_bytes(tile);
-    if (force_only) k_force<kF32, true><<<d.ntiles, tile, sm, s>>>(d, Yin, Xout, tile);
-    else k_force<kF32, false><<<d.ntiles, tile, sm, s>>>(d, Yin, Xout, tile);
+    if (force_only) k_force_lists<true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    else k_force_lists<false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    k_force_pairs<<<d.ntiles, kPairChunks * tile, force_smem_bytes(kPairChunks * tile), s>>>(d, Xout, tile);
   } else {
-    if (force_only) k_force<kF64, true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
-    else k_force<kF64, false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    if (force_only) k_force_f64<true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    else k_force_f64<false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
   }
 }
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s) {

@@ -25,6 +25,8 @@ enum Prec : int { kF32 = 0, kF64 = 1 };
 void launch_pack(const DevPtrs& d, int prec, int tile, cudaStream_t s);
 void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, bool mid, int tile,
                            int prec, cudaStream_t s);
+// Largest force tile (molecules per block) of a precision: FP32 blocks hold two threads per molecule.
+int max_force_tile(int prec);
 // Kernel attributes the force launches need (call once per device before launching).
 cudaError_t force_kernel_setup();
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,

@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kNoAllocMaxMol = 2048;
 constexpr int kNoAllocMaxNbr = 1024;
-constexpr int kNoAllocTile = 128;
+constexpr int kNoAllocTile = 64;
 constexpr int kNoAllocMaxTiles = kNoAllocMaxMol / kNoAllocTile;
 constexpr double kNoAllocSkin = 1.0;
 
@@ -48,7 +48,8 @@ constexpr size_t kOffRef = kOffPack + al(4 * 20 * kNoAllocMaxMol);
 constexpr size_t kOffLb = kOffRef + al(sizeof(int4) * kNoAllocMaxMol);
 constexpr size_t kOffNbr = kOffLb + al(8 * 3 * kNoAllocMaxTiles);
 constexpr size_t kOffNbt = kOffNbr + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
-constexpr size_t kOffCnt = kOffNbt + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
+constexpr size_t kOffNtc = kOffNbt + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
+constexpr size_t kOffCnt = kOffNtc + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffPart = kOffCnt + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * (kNoAllocMaxMol / 32));
 constexpr size_t kScratchBytes = kOffErr + al(16);
@@ -192,6 +193,7 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   d.Lbuild = reinterpret_cast<double*>(b + kOffLb);
   d.nbr = reinterpret_cast<uint16_t*>(b + kOffNbr);
   d.nbt = reinterpret_cast<uint16_t*>(b + kOffNbt);
+  d.nt_cnt = reinterpret_cast<int*>(b + kOffNtc);
   d.nbr_cnt = reinterpret_cast<int*>(b + kOffCnt);
   d.wall = d_wall;
   d.part1 = nullptr;

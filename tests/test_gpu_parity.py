@@ -341,7 +341,7 @@ def test_tile_and_skin_do_not_change_the_trajectory():
     bit-identical averages."""
     ens = _tuning_batch()
     runs = []
-    for tuning in [None, (32, 0.6), (96, 1.4)]:
+    for tuning in [None, (32, 0.6), (32, 1.4)]:
         eng = E.REMDGPU(ens, precision="fp32")
         if tuning:
             eng.set_tuning(*tuning)
