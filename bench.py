@@ -583,6 +583,7 @@ def engine_arm(args, rank, world, local):
     local_ms = float(sum(ms))
     value, max_ms, total_units = aggregate(local_ms, mol_steps_per_interval * args.steps, world)
     statuses = [eng.replica_status(r) for r in range(eng.nrep)]
+    launches = eng.launches_per_interval() * args.steps   # with the device exchange, as timed
 
     # roofline of the force kernel: per-launch algorithmic FLOPs / event duration
     eng.compute_forces()
@@ -601,7 +602,9 @@ def engine_arm(args, rank, world, local):
     peak = ctypes.c_double()
     E._check(E.lib().remd_measure_fp32_peak(dev, ctypes.byref(peak)))
     achieved = flops / (force_ms * 1e-3) / 1e12
-    roof = {"bound": "fp32", "kernel": "k_force (pair loop + wall + A2M)",
+    roof = {"bound": "fp32",
+            "kernel": "force step: k_force_lists (head, list rebuild, pairs within rcut) + "
+                      "k_force_pairs (pair forces, wall, A2M)",
             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value,
             "peak_source": "measured: register-resident FP32 FMA chains on all SMs "
@@ -674,7 +677,7 @@ def engine_arm(args, rank, world, local):
                 "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": dict(workload_desc(args.config, ens, args.interval), tuning=tuning),
-                "gpu_launches": eng.launches_per_interval() * args.steps,
+                "gpu_launches": launches,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
                 "latency": {"p50_interval_ms": float(np.percentile(ms, 50)),
                             "p99_interval_ms": float(np.percentile(ms, 99)),
