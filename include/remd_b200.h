@@ -192,7 +192,7 @@ remd_status remd_measure_fp32_peak(int device, double *tflops);
 remd_status remd_replica_status(remd_handle h, int rep, int *status);
 
 /* Tuning: molecules of one force tile (multiple of 32: 32..64 for FP32 handles,
- * 32..128 for FP64; defaults 64 / 128) and the neighbour
+ * 32..128 for FP64; defaults 32 / 128) and the neighbour
  * skin (A).  Takes effect on the next call. */
 remd_status remd_set_tuning(remd_handle h, int tile, double skin);
 

@@ -167,6 +167,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       (h->prec == kF32) ? (size_t)nbr_words * 2 : 0,   // 30 nbt (FP32 per-step lists)
       nt * 4,                          // 31 order
       (h->prec == kF32) ? N * 4 : 0,   // 32 nt_cnt (FP32 per-step list counts)
+      N * sizeof(int4),                // 33 com (FP32 current fixed-point centres)
   };
   offs.clear();
   total = 0;
@@ -229,6 +230,7 @@ static remd_status allocate(remd_engine_s* h) {
   d.nbt = reinterpret_cast<uint16_t*>(b + offs[30]);
   d.order = reinterpret_cast<int*>(b + offs[31]);
   d.nt_cnt = reinterpret_cast<int*>(b + offs[32]);
+  d.com = reinterpret_cast<int4*>(b + offs[33]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
@@ -391,7 +393,7 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   auto* h = new remd_engine_s;
   h->device = device;
   h->prec = (prec == REMD_PREC_FP64) ? kF64 : kF32;
-  h->tile = max_force_tile(h->prec);   // 64 (FP32), 128 (FP64); remd_set_tuning / remd_autotune change it
+  h->tile = (h->prec == kF32) ? 32 : 128;   // measured best on config 4; remd_set_tuning / remd_autotune change it
   h->nens = nens;
   h->interval = systems[0].interval;
   h->sys.assign(systems, systems + nens);

@@ -90,6 +90,7 @@ struct DevPtrs {
   double *r, *v, *q, *p, *f, *n; // SoA, component-major, stride N
   void* pack;                    // FP32 words or FP64 doubles
   int4* ref_com;                 // fixed-point com at the last list build
+  int4* com;                     // FP32 form: current fixed-point com (written with the pack)
   double* Lbuild;                // per tile, 3 doubles (NaN = list invalid)
   uint16_t* nbr;                 // neighbour lists (rcut + skin)
   uint16_t* nbt;                 // FP32 form: per-step lists of the pairs within rcut (same layout)

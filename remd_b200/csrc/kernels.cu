@@ -77,6 +77,10 @@ __device__ inline void reduce_part2(const DevPtrs& d, const RepConst& c, double&
   vir[0] = v0 * 0.5; vir[1] = v1 * 0.5; vir[2] = v2 * 0.5;
 }
 
+// Difference of two fixed-point box fractions with 32-bit wraparound: the
+// minimum-image separation in units of L / 2^32 (defined via unsigned arithmetic).
+__device__ __forceinline__ int wrap_diff(int a, int b) { return (int)((unsigned)a - (unsigned)b); }
+
 // ------------------------------------------------------------------ force records
 __device__ inline int fix_coord(double r) {
   // box fraction in [0,1) -> (r-0.5)*2^32 as a wrapping int32
@@ -101,6 +105,7 @@ __device__ inline void write_pack(const DevPtrs& d, const RepConst& c, int prec,
     uint4* w4 = reinterpret_cast<uint4*>(w);
     for (int k = 0; k < c.pack_stride / 4; k++)
       w4[k] = make_uint4(buf[4 * k], buf[4 * k + 1], buf[4 * k + 2], buf[4 * k + 3]);
+    d.com[c.mol_off + li] = make_int4((int)buf[0], (int)buf[1], (int)buf[2], 0);
   } else {
     double* w = reinterpret_cast<double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
     w[0] = r[0]; w[1] = r[1]; w[2] = r[2];
@@ -210,9 +215,9 @@ __global__ void __launch_bounds__(256) k_integrate(DevPtrs d, const RepState* __
     // displacement since the last neighbour-list build, in the build box
     const int4 ref = d.ref_com[g];
     const int fx = fix_coord(r[0]), fy = fix_coord(r[1]), fz = fix_coord(r[2]);
-    const double dx = (double)(int)(fx - ref.x) * kFixInv * sc.Lb[0];
-    const double dy = (double)(int)(fy - ref.y) * kFixInv * sc.Lb[1];
-    const double dz = (double)(int)(fz - ref.z) * kFixInv * sc.Lb[2];
+    const double dx = (double)wrap_diff(fx, ref.x) * kFixInv * sc.Lb[0];
+    const double dy = (double)wrap_diff(fy, ref.y) * kFixInv * sc.Lb[1];
+    const double dz = (double)wrap_diff(fz, ref.z) * kFixInv * sc.Lb[2];
     disp = sqrt(dx * dx + dy * dy + dz * dz);
     if (!(disp == disp)) disp = 1e30;   // NaN box: force a rebuild
   }
@@ -263,8 +268,7 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
     for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) {
       const long long off = c.pack_off + (long long)(base + k) * c.pack_stride;
       if (PREC == kF32) {
-        const int* w = reinterpret_cast<const int*>(d.pack) + off;
-        reinterpret_cast<int4*>(&cand[k])[0] = make_int4(w[0], w[1], w[2], 0);
+        reinterpret_cast<int4*>(&cand[k])[0] = d.com[c.mol_off + base + k];
       } else {
         const double* w = reinterpret_cast<const double*>(d.pack) + off;
         cand[k] = make_double4(w[0], w[1], w[2], 0);
@@ -278,9 +282,9 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
         double dx, dy, dz;
         if (PREC == kF32) {
           const int4 cj = reinterpret_cast<const int4*>(&cand[k])[0];
-          dx = (double)(int)(ix - cj.x) * kFixInv * L[0];
-          dy = (double)(int)(iy - cj.y) * kFixInv * L[1];
-          dz = (double)(int)(iz - cj.z) * kFixInv * L[2];
+          dx = (double)wrap_diff(ix, cj.x) * kFixInv * L[0];
+          dy = (double)wrap_diff(iy, cj.y) * kFixInv * L[1];
+          dz = (double)wrap_diff(iz, cj.z) * kFixInv * L[2];
         } else {
           const double4 cj = cand[k];
           dx = (rx - cj.x) * L[0];
@@ -371,9 +375,9 @@ __device__ __noinline__ void site_pair_exact(const DevPtrs& d, const RepConst& c
   const int stride = c.pack_stride;
   const int* wi = reinterpret_cast<const int*>(base + (long long)li * stride);
   const int* wj = reinterpret_cast<const int*>(base + (long long)j * stride);
-  const float dx = (float)(int)(wi[0] - wj[0]) * k32.Ls[0];
-  const float dy = (float)(int)(wi[1] - wj[1]) * k32.Ls[1];
-  const float dz = (float)(int)(wi[2] - wj[2]) * k32.Ls[2];
+  const float dx = (float)wrap_diff(wi[0], wj[0]) * k32.Ls[0];
+  const float dy = (float)wrap_diff(wi[1], wj[1]) * k32.Ls[1];
+  const float dz = (float)wrap_diff(wi[2], wj[2]) * k32.Ls[2];
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2);
   const float r = r2 * rinv;
@@ -437,12 +441,11 @@ template <bool SIMG>
 __device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, const double* L,
                                 const uint16_t* nb, uint16_t* nt, int cnt) {
   const int T = blockDim.x;
-  const int nv = c.pack_stride / 4;   // uint4 per record
-  const uint4* base = reinterpret_cast<const uint4*>(reinterpret_cast<const uint32_t*>(d.pack) + c.pack_off);
+  const int4* base = d.com + c.mol_off;   // compact centres: 16 B per molecule, L1-resident
   const float Ls0 = (float)(L[0] * kFixInv), Ls1 = (float)(L[1] * kFixInv), Ls2 = (float)(L[2] * kFixInv);
   const float rc2 = (float)(c.rc * c.rc);
-  const uint4 ui = __ldg(base + (long long)li * nv);
-  const int xi = (int)ui.x, yi = (int)ui.y, zi = (int)ui.z;
+  const int4 ui = __ldg(base + li);
+  const int xi = ui.x, yi = ui.y, zi = ui.z;
   // far bound: |d_x| below it keeps every site-pair component below L/2 - kImageTol
   float bnd0 = 0.f, bnd1 = 0.f, bnd2 = 0.f;
   if (SIMG) {
@@ -466,21 +469,20 @@ __device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, con
   int k = 0;
   for (; k + B <= cnt; k += B) {
     int j[B];
-    uint4 u[B];
+    int4 u[B];
 #pragma unroll
     for (int m = 0; m < B; m++) j[m] = nb[(long long)(k + m) * T];
 #pragma unroll
-    for (int m = 0; m < B; m++) u[m] = __ldg(base + (long long)j[m] * nv);
+    for (int m = 0; m < B; m++) u[m] = __ldg(base + j[m]);
 #pragma unroll
     for (int m = 0; m < B; m++)
-      keep(j[m], (float)(int)(xi - (int)u[m].x) * Ls0, (float)(int)(yi - (int)u[m].y) * Ls1,
-           (float)(int)(zi - (int)u[m].z) * Ls2);
+      keep(j[m], (float)wrap_diff(xi, u[m].x) * Ls0, (float)wrap_diff(yi, u[m].y) * Ls1,
+           (float)wrap_diff(zi, u[m].z) * Ls2);
   }
   for (; k < cnt; k++) {
     const int j = nb[(long long)k * T];
-    const uint4 u = __ldg(base + (long long)j * nv);
-    keep(j, (float)(int)(xi - (int)u.x) * Ls0, (float)(int)(yi - (int)u.y) * Ls1,
-         (float)(int)(zi - (int)u.z) * Ls2);
+    const int4 u = __ldg(base + j);
+    keep(j, (float)wrap_diff(xi, u.x) * Ls0, (float)wrap_diff(yi, u.y) * Ls1, (float)wrap_diff(zi, u.z) * Ls2);
   }
   d.nt_cnt[c.mol_off + li] = nfar | (nnear << 16);
 }
@@ -568,9 +570,9 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const F32Cons
 #pragma unroll
         for (int m = 0; m < NV; m++) nx[m] = __ldg(base + (long long)jn * NV + m);
       }
-      const float dx = (float)(int)(xi - (int)wj[0]) * Ls0;
-      const float dy = (float)(int)(yi - (int)wj[1]) * Ls1;
-      const float dz = (float)(int)(zi - (int)wj[2]) * Ls2;
+      const float dx = (float)wrap_diff(xi, (int)wj[0]) * Ls0;
+      const float dy = (float)wrap_diff(yi, (int)wj[1]) * Ls1;
+      const float dz = (float)wrap_diff(zi, (int)wj[2]) * Ls2;
       const float r2 = dx * dx + dy * dy + dz * dz;
       const float rinv = rsqrtf(r2);
       const float r = r2 * rinv;
@@ -989,7 +991,7 @@ __global__ void __launch_bounds__(128) k_force_f64(DevPtrs d, const RepState* __
 // FP32 form, first launch of a step: head, skin-list rebuild when due, pass 1.
 // Light on registers, so many warps hide the gathered loads of pass 1.
 template <bool FORCE_ONLY>
-__global__ void __launch_bounds__(128, 8) k_force_lists(DevPtrs d, const RepState* __restrict__ Yin,
+__global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepState* __restrict__ Yin,
                                                      RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
   const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;

@@ -49,7 +49,8 @@ constexpr size_t kOffLb = kOffRef + al(sizeof(int4) * kNoAllocMaxMol);
 constexpr size_t kOffNbr = kOffLb + al(8 * 3 * kNoAllocMaxTiles);
 constexpr size_t kOffNbt = kOffNbr + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
 constexpr size_t kOffNtc = kOffNbt + al(2 * (size_t)kNoAllocMaxNbr * kNoAllocTile * kNoAllocMaxTiles);
-constexpr size_t kOffCnt = kOffNtc + al(4 * kNoAllocMaxMol);
+constexpr size_t kOffCom = kOffNtc + al(4 * kNoAllocMaxMol);
+constexpr size_t kOffCnt = kOffCom + al(sizeof(int4) * kNoAllocMaxMol);
 constexpr size_t kOffPart = kOffCnt + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * (kNoAllocMaxMol / 32));
 constexpr size_t kScratchBytes = kOffErr + al(16);
@@ -194,6 +195,7 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   d.nbr = reinterpret_cast<uint16_t*>(b + kOffNbr);
   d.nbt = reinterpret_cast<uint16_t*>(b + kOffNbt);
   d.nt_cnt = reinterpret_cast<int*>(b + kOffNtc);
+  d.com = reinterpret_cast<int4*>(b + kOffCom);
   d.nbr_cnt = reinterpret_cast<int*>(b + kOffCnt);
   d.wall = d_wall;
   d.part1 = nullptr;
