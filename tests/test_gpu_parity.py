@@ -292,6 +292,25 @@ def test_fp32_accuracy_tip5p_bulk_1728():
     assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
 
 
+@pytest.mark.parametrize("model,confined,wall,rc", [("tip5p", 0, 0.0, 12.0), ("tip4p", 1, 7.0, 10.0),
+                                                   ("tip3p", 2, 12.0, 11.0)])
+def test_fp32_accuracy_large_systems(model, confined, wall, rc):
+    """The largest systems of the serving stream (N = 4096: a 50 A bulk box, a
+    1.4 um nanotube, a 115 A slit): FP32 forces, torques and energy against the
+    FP64 oracle at the same gates as the liquid-density batch."""
+    e = S.make_ensemble("big", model, confined, 4096, wall, rc, rc - 1.0, 1, 1, 300, 300, 0.1e6, 0.1e6, 41)
+    st = e.states[0]
+    eng = E.REMDGPU([single(e.spec, st)], precision="fp32")
+    g = eng.ConvertVariablesToHost(0)
+    orc = O.Oracle(e.spec, st)
+    orc.initialize_property()
+    assert rel(g["f"], orc.f) < 1e-5
+    assert rel(g["n"], orc.n) < 1e-5
+    assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
+    assert abs(eng.pair_count() - orc.prop()["npairs"]) <= 2
+    eng.close()
+
+
 def _simg_tie_case():
     z = np.load(os.path.join(GOLDEN, "simg_tie.npz"))
     e = S.make_ensemble("tie", "tip3p", 0, len(z["r"]), 0.0, float(z["rcut"]), float(z["rswitch"]),
