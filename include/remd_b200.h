@@ -253,6 +253,14 @@ remd_status remd_read_chk(const char *path, int nmol, double *r, double *v, doub
                           double *mass, double *inertia, double *scal);
 /* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) of replica rep. */
 remd_status remd_write_chk(remd_handle h, int rep, const char *path);
+/* The .gro output of replica rep as IOManager::UpdateOutputs writes it
+ * (src/io_manager.cxx:636-651 -> ConvertMoleculesToAtoms 797-814 ->
+ * write_gro_file, src/gro.cxx:118-135): comment "test", site coordinates
+ * r L + R(q) b in nm, velocities 0, box in nm.  The molecule and site names
+ * (moltype.txt; the engine does not keep them) are padded to 5 characters like
+ * MakeMolTypeList does (src/molecules.cxx:86, 95). */
+remd_status remd_write_gro(remd_handle h, int rep, const char *path, const char *mol_name,
+                           const char *const *atom_names);
 
 /* Force snapshot of one replica that allocates nothing.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory -- a host

@@ -244,6 +244,47 @@ def replica_exchange(ntemp, npress, pconstant, step, index, T, P, pot, vol, u):
 _REFLIBS = {}
 
 
+def gro_atoms(mol_name, atom_names, r, q, L, body):
+    """IOManager::ConvertMoleculesToAtoms (src/io_manager.cxx:797-814): per site,
+    molecule id i+1, the names padded as MakeMolTypeList pads them
+    (src/molecules.cxx:86, 95), atom id, coordinates (r L + R(q) b) in nm.
+    r (n,3) box fractions, q (n,4), L (3,) and body (k,3) in A."""
+    from remd_b200.systems import body_to_space
+    n, k = len(r), len(body)
+    mname = mol_name.ljust(5)
+    anames = [a.rjust(5) for a in atom_names]
+    sites = body_to_space(np.asarray(q, dtype=float), np.asarray(body, dtype=float))   # (n,k,3)
+    coor = (np.asarray(r, dtype=float)[:, None, :] * np.asarray(L, dtype=float) + sites) * 0.1
+    molid = np.repeat(np.arange(1, n + 1), k)
+    return molid, [mname] * (n * k), anames * n, np.arange(1, n * k + 1), coor.reshape(-1, 3)
+
+
+def gro_text(molid, molname, atomname, atomid, coor, L, comment="test"):
+    """write_gro_file (src/gro.cxx:118-135) as text: comment, atom count, one
+    "%5d%s%s%5d%8.3f%8.3f%8.3f%8.4f%8.4f%8.4f" line per atom (velocities 0),
+    the box "%10.5f%10.5f%10.5f"."""
+    out = [comment, "%5d" % len(molid)]
+    for m, mn, an, a, c in zip(molid, molname, atomname, atomid, coor):
+        out.append("%5d%s%s%5d%8.3f%8.3f%8.3f%8.4f%8.4f%8.4f" % (m, mn, an, a, c[0], c[1], c[2],
+                                                               0.0, 0.0, 0.0))
+    out.append("%10.5f%10.5f%10.5f" % tuple(L))
+    return "\n".join(out) + "\n"
+
+
+def reference_write_gro(path, molid, molname, atomname, atomid, coor, L, comment="test"):
+    """The reference's own write_gro_file (src/gro.cxx:118-135, compiled into
+    oracle/_ref) on the same atoms."""
+    lib = _ref_lib()
+    n = len(molid)
+    enc = lambda xs: (C.c_char_p * n)(*[x.encode() for x in xs])  # noqa: E731
+    mi = np.ascontiguousarray(molid, dtype=np.int32)
+    ai = np.ascontiguousarray(atomid, dtype=np.int32)
+    cc = np.ascontiguousarray(coor, dtype=float)
+    LL = np.ascontiguousarray(L, dtype=float)
+    lib.ref_write_gro(path.encode(), C.c_int(n), _ptr(mi, _ip), enc(molname), enc(atomname),
+                      _ptr(ai, _ip), _ptr(cc), _ptr(LL), comment.encode())
+
+
 def reference_available(variant="generic"):
     return os.path.exists(_ref_path(variant))
 
@@ -273,6 +314,8 @@ def _ref_lib(variant="generic"):
         lib.ref_remdinfo_exchange.restype = C.c_int
         lib.ref_remdinfo_exchange.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _ip]
         lib.ref_remdinfo_arrays.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        lib.ref_write_gro.argtypes = [C.c_char_p, C.c_int, _ip, C.POINTER(C.c_char_p),
+                                      C.POINTER(C.c_char_p), _ip, _dp, _dp, C.c_char_p]
         for fn in ["ref_set_state", "ref_get_state", "ref_get_property", "ref_get_average",
                    "ref_get_fwall"]:
             getattr(lib, fn).argtypes = None

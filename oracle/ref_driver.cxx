@@ -9,9 +9,11 @@
 // (it needs the unvendored VMD molfile plugin), so the caller passes the state
 // arrays already converted the way ReadCheckPoint converts them: r as a box
 // fraction, v scaled by L*s, p scaled by s.
+#include "gro.h"
 #include "molecules.h"
 #include "remdinfo.h"
 
+#include <cstdio>
 #include <cstring>
 #include <sstream>
 #include <string>
@@ -208,6 +210,27 @@ int ref_remdinfo_exchange(void* h, long step, const double* pot, const double* v
     }
   }
   return len;
+}
+
+// The reference's .gro writer (src/gro.cxx:118-135) on atoms given as arrays:
+// molecule id, molecule name, atom name, atom id, coordinates (nm); velocities 0.
+void ref_write_gro(const char* path, int natom, const int* molid, const char* const* molname,
+                   const char* const* atomname, const int* atomid, const double* coor, const double* L,
+                   const char* comment) {
+  std::vector<AtomGro> a(natom);
+  for (int i = 0; i < natom; i++) {
+    std::snprintf(a[i].MolName, sizeof(a[i].MolName), "%s", molname[i]);
+    std::snprintf(a[i].AtomName, sizeof(a[i].AtomName), "%s", atomname[i]);
+    a[i].MolID = molid[i];
+    a[i].AtomID = atomid[i];
+    for (int d = 0; d < 3; d++) {
+      a[i].coor[d] = coor[3 * i + d];
+      a[i].vel[d] = 0.0;
+    }
+  }
+  dvec3 box;
+  for (int d = 0; d < 3; d++) box[d] = L[d];
+  write_gro_file(path, natom, a.data(), box, comment);
 }
 
 }  // extern "C"

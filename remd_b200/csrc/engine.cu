@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -12,6 +13,7 @@
 #include "../../include/remd_b200.h"
 #include "engine_types.cuh"
 #include "hostio.h"
+#include "integrator.cuh"
 #include "kernels.cuh"
 
 using namespace remd;
@@ -937,6 +939,61 @@ remd_status remd_write_chk(remd_handle h, int rep, const char* path) {
   if (s != REMD_OK) return s;
   return (remd_status)write_chk(path, n, c.nsite, r.data(), v.data(), q.data(), p.data(), c.mass, c.I,
                                 o.s, o.Ps, o.Q, o.Pv, o.W, o.L);
+}
+
+remd_status remd_write_gro(remd_handle h, int rep, const char* path, const char* mol_name,
+                           const char* const* atom_names) {
+  if (!h || !path || !mol_name || !atom_names || rep < 0 || rep >= h->nrep) return REMD_ERR_INVALID;
+  const RepConst& c = h->rc[rep];
+  const int n = c.nmol, ns = c.nsite;
+  for (int k = 0; k < ns; k++)
+    if (!atom_names[k]) return REMD_ERR_INVALID;
+  std::vector<double> r(3 * n), q(4 * n);
+  remd_state_view o;
+  std::memset(&o, 0, sizeof(o));
+  o.r = r.data(); o.q = q.data();
+  remd_status s = remd_get_state(h, rep, &o);
+  if (s != REMD_OK) return s;
+  // names as MakeMolTypeList pads them (src/molecules.cxx:86, 95): the molecule
+  // name left-justified, the atom names right-justified, to 5 characters
+  std::string mname(mol_name);
+  while (mname.size() < 5) mname += " ";
+  std::vector<std::string> anames(ns);
+  for (int k = 0; k < ns; k++) {
+    anames[k] = atom_names[k];
+    while (anames[k].size() < 5) anames[k] = " " + anames[k];
+  }
+  FILE* fp = std::fopen(path, "w");
+  if (!fp) {
+    set_error(std::string("remd_write_gro: cannot open ") + path);
+    return REMD_ERR_IO;
+  }
+  // IOManager::ConvertMoleculesToAtoms (src/io_manager.cxx:797-814): site = r L + R(q) b,
+  // angstrom -> nm, velocities written as zero; write_gro_file (src/gro.cxx:118-135)
+  // with the comment and the box in nm of IOManager::UpdateOutputs (src/io_manager.cxx:636-651)
+  const double A_to_nm = 0.1;
+  std::fprintf(fp, "%s\n", "test");
+  std::fprintf(fp, "%5d\n", n * ns);
+  int count = 0;
+  for (int i = 0; i < n; i++) {
+    const double qi[4] = {q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+    for (int k = 0; k < ns; k++) {
+      double sk[3];
+      body_to_space(qi, c.body[k], sk);
+      double x[3];
+      for (int d = 0; d < 3; d++) x[d] = (r[3 * i + d] * o.L[d] + sk[d]) * A_to_nm;
+      count++;
+      std::fprintf(fp, "%5d%s%s%5d%8.3lf%8.3lf%8.3lf%8.4lf%8.4lf%8.4lf\n", i + 1, mname.c_str(),
+                   anames[k].c_str(), count, x[0], x[1], x[2], 0.0, 0.0, 0.0);
+    }
+  }
+  std::fprintf(fp, "%10.5lf%10.5lf%10.5lf\n", o.L[0] * A_to_nm, o.L[1] * A_to_nm, o.L[2] * A_to_nm);
+  const bool ok = std::fclose(fp) == 0;
+  if (!ok) {
+    set_error(std::string("remd_write_gro: write failed: ") + path);
+    return REMD_ERR_IO;
+  }
+  return REMD_OK;
 }
 
 }  // extern "C"

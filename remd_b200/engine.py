@@ -120,6 +120,8 @@ def lib():
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]
         L.remd_write_chk.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+        L.remd_write_gro.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p,
+                                     C.POINTER(C.c_char_p)]
         L.remd_wall_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, _dp]
         L.remd_read_chk.argtypes = [C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -421,6 +423,12 @@ class REMDGPU:
 
     def write_chk(self, rep, path):
         _check(lib().remd_write_chk(self.h, rep, path.encode()))
+
+    def write_gro(self, rep, path, moltype):
+        """The reference's .gro output of replica rep (remd_write_gro); names from
+        the molecule type."""
+        names = (C.c_char_p * moltype.nsite)(*[a.encode() for a in moltype.names])
+        _check(lib().remd_write_gro(self.h, rep, path.encode(), moltype.name.encode(), names))
 
 
 def force_snapshot_noalloc(spec, d_r, d_q, L, d_wall, d_f, d_n, d_out, stream=None):

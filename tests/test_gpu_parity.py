@@ -408,3 +408,24 @@ def test_graph_exchange_equals_explicit_exchange():
         assert sorted(ia[off:off + e.nreplica]) == list(range(e.nreplica))
         assert np.array_equal(np.sort(Ta[off:off + e.nreplica]), np.sort(e.T))
         off += e.nreplica
+
+
+def test_write_gro_matches_reference_writer(tmp_path):
+    """remd_write_gro of an advanced replica gives the bytes the reference's
+    IOManager::UpdateOutputs path writes for the same state (restated
+    ConvertMoleculesToAtoms, the reference's own write_gro_file when built)."""
+    e = S.small_ensemble("tip4p", 2, nmol=90, ntemp=1, npress=1, seed=23, interval=10)
+    eng = E.REMDGPU([e], precision="fp32")
+    eng.ExecuteSteps(e.T, e.P)
+    path = str(tmp_path / "engine.gro")
+    mt = e.spec.moltype
+    eng.write_gro(0, path, mt)
+    g = eng.ConvertVariablesToHost(0)
+    atoms = O.gro_atoms(mt.name, mt.names, g["r"], g["q"], g["L"], mt.r)
+    text = O.gro_text(*atoms, L=g["L"] * 0.1)
+    assert open(path).read() == text
+    if O.reference_available():
+        ref = str(tmp_path / "ref.gro")
+        O.reference_write_gro(ref, *atoms, L=g["L"] * 0.1)
+        assert open(ref).read() == text
+    eng.close()

@@ -96,3 +96,21 @@ def test_exchange_matches_reference_remdinfo():
         assert np.array_equal(acc_o, acc_r[:len(acc_o)])
         assert np.array_equal(idx_o, idx_r)
         assert np.array_equal(T_o, T_r) and np.array_equal(P_o, P_r)
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref not built (no reference sources)")
+def test_gro_restatement_matches_reference_writer(tmp_path):
+    """The .gro restatement (ConvertMoleculesToAtoms + write_gro_file) gives the
+    same bytes as the reference's own writer on the same atoms, including
+    coordinates that round at the last printed digit and negative ones."""
+    from remd_b200 import systems as S
+    e = S.small_ensemble("tip5p", 1, nmol=40, ntemp=1, npress=1, seed=17)
+    st, mt = e.states[0], e.spec.moltype
+    atoms = O.gro_atoms(mt.name, mt.names, st.r, st.q, st.L, mt.r)
+    text = O.gro_text(*atoms, L=st.L * 0.1)
+    path = str(tmp_path / "ref.gro")
+    O.reference_write_gro(path, *atoms, L=st.L * 0.1)
+    assert open(path).read() == text
+    lines = text.splitlines()
+    assert lines[0] == "test" and int(lines[1]) == 40 * 5 and len(lines) == 40 * 5 + 3
+    assert lines[2][5:15] == "TIP5P   OW"
