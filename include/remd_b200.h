@@ -73,7 +73,10 @@ typedef struct {
   double site_sigma[REMD_MAX_SITES];
   double site_eps[REMD_MAX_SITES];
   double site_charge[REMD_MAX_SITES];
-  int tconstant;            /* 0 NVE-like, 1 Nose-Poincare                       */
+  int tconstant;            /* 0 NVE-like, 1 Nose-Poincare, 2 velocity scaling  */
+                            /* before every step (bulk pconstant 0; tube         */
+                            /* pconstant 0 or 2: Molecules::ExecuteSteps,        */
+                            /* src/integrator.cxx:713-787)                       */
   int pconstant;            /* 0 none, 1 3-D, 2 z (tube), 3 xy (slit)            */
   int confined;             /* 0 bulk, 1 nanotube, 2 nano-slit                   */
   double dt_fs;

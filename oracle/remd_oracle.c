@@ -605,7 +605,15 @@ void orc_get_average(const orc_system *sys, const orc_replica *rep, double out[O
 }
 
 void orc_execute_steps(const orc_system *sys, orc_replica *rep, int nsteps) {
-  for (int s = 0; s < nsteps; s++) orc_step(sys, rep);
+  /* Molecules::ExecuteSteps (src/integrator.cxx:708-723): the velocity-scaling
+     thermostat (tconstant 2) rescales before every step */
+  for (int s = 0; s < nsteps; s++) {
+    if (TMODE(sys) == 2) {
+      orc_velocity_scaling(sys, rep);
+      orc_ang_velocity_scaling(sys, rep);
+    }
+    orc_step(sys, rep);
+  }
   orc_calc_properties(sys, rep);
 }
 
@@ -663,7 +671,7 @@ void orc_kill_momentum(const orc_system *sys, orc_replica *rep) {
 }
 
 void orc_velocity_scaling(const orc_system *sys, orc_replica *rep) {
-  /* src/molecules.cxx:262-275 */
+  /* src/molecules.cxx:261-273 */
   double k[3];
   translational_energy(sys, rep, k);
   const double tra = k[0] + k[1] + k[2];
@@ -678,7 +686,7 @@ void orc_velocity_scaling(const orc_system *sys, orc_replica *rep) {
 }
 
 void orc_ang_velocity_scaling(const orc_system *sys, orc_replica *rep) {
-  /* src/molecules.cxx:293-307 */
+  /* src/molecules.cxx:296-311 */
   const double rot = rotational_energy(sys, rep);
   if (rot == 0.) return;
   const double coef = sqrt(1.5 * sys->nmol * rep->T / rot);

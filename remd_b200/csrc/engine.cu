@@ -55,6 +55,7 @@ struct remd_engine_s {
   int graph_tile = 0;
   bool graph_exchange = false;
   bool exch_enabled = false;        // device exchange appended to every interval
+  bool vscale = false;              // some replica uses velocity scaling (tconstant 2)
   unsigned long long exch_seed = 0;
   long long* d_step = nullptr;      // per-ensemble interval counter of the device exchange
   unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
@@ -87,7 +88,15 @@ static remd_status check_desc(const remd_system_desc& s, std::string& why) {
           "(TIP3P/TIP4P/TIP5P layout)";
     return REMD_ERR_INVALID;
   }
-  if (s.tconstant < 0 || s.tconstant > 1) { why = "tconstant must be 0 or 1"; return REMD_ERR_INVALID; }
+  if (s.tconstant < 0 || s.tconstant > 2) { why = "tconstant must be 0, 1 or 2"; return REMD_ERR_INVALID; }
+  // velocity scaling: the modes Molecules::ExecuteSteps integrates (src/integrator.cxx:730-787:
+  // NVTSCALE, NVTSCALE1D, NAxyPzTSCALE1D); the other *TSCALE* modes fall through its switch
+  // and are not integrated at all there, so they are rejected here
+  if (s.tconstant == 2 && !((s.confined == 0 && s.pconstant == 0) ||
+                            (s.confined == 1 && (s.pconstant == 0 || s.pconstant == 2)))) {
+    why = "tconstant 2 (velocity scaling) is integrated for bulk pconstant 0 and tube pconstant 0 or 2 only";
+    return REMD_ERR_INVALID;
+  }
   if (s.pconstant < 0 || s.pconstant > 3) { why = "pconstant must be 0..3"; return REMD_ERR_INVALID; }
   if (s.confined < 0 || s.confined > 2) { why = "confined must be 0..2"; return REMD_ERR_INVALID; }
   // src/remd.cxx:35-36
@@ -282,13 +291,29 @@ static remd_status initial_force(remd_engine_s* h) {
   return sync_and_check(h);
 }
 
+// The integrate part of MD step s of an interval.  With velocity-scaling
+// replicas (tconstant 2) every step first closes the previous one
+// (k_replica_end: the last half kick), rescales the velocities of those replicas
+// (VelocityScaling + AngVelocityScaling before every step, as
+// Molecules::ExecuteSteps does, src/integrator.cxx:713-723) and opens the step;
+// the other replicas' arithmetic is the same as in the fused closing + opening.
+static void launch_step_integrate(remd_engine_s* h, int s) {
+  if (h->vscale) {
+    if (s > 0) launch_replica_end(h->d, h->X, h->stream);
+    launch_replica_rescale(h->d, h->X, true, h->stream);
+    launch_integrate_prec(h->d, h->X, h->Y, false, h->tile, h->prec, h->stream);
+  } else {
+    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+  }
+}
+
 static remd_status build_graph(remd_engine_s* h) {
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   launch_replica_start(h->d, h->X, h->stream);
   for (int s = 0; s < h->interval; s++) {
-    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    launch_step_integrate(h, s);
     launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
   }
   launch_replica_end(h->d, h->X, h->stream);
@@ -448,6 +473,7 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
       c.c0 = c0;
       c.confined = s.confined;
       c.tconstant = s.tconstant;
+      if (s.tconstant == 2) h->vscale = true;
       c.pconstant = s.pconstant;
       c.nfwall = s.nfwall;
       c.wall_off = wall_off[e];
@@ -716,7 +742,7 @@ remd_status remd_execute_nsteps(remd_handle h, int nsteps) {
   if (!h || nsteps < 1) { set_error("remd_execute_nsteps: nsteps must be >= 1"); return REMD_ERR_INVALID; }
   launch_replica_start(h->d, h->X, h->stream);
   for (int s = 0; s < nsteps; s++) {
-    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    launch_step_integrate(h, s);
     launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
   }
   launch_replica_end(h->d, h->X, h->stream);
@@ -726,7 +752,7 @@ remd_status remd_execute_nsteps(remd_handle h, int nsteps) {
 
 remd_status remd_rescale_velocities(remd_handle h) {
   if (!h) return REMD_ERR_INVALID;
-  launch_replica_rescale(h->d, h->X, h->stream);
+  launch_replica_rescale(h->d, h->X, false, h->stream);
   CK(cudaGetLastError());
   return sync_and_check(h);
 }
@@ -800,10 +826,12 @@ long long remd_last_pair_count(remd_handle h) {
   return h->last_pairs;
 }
 int remd_launches_per_interval(remd_handle h) {
-  // replica_start + per MD step (integrate, force: lists + pairs in FP32, one launch in FP64)
+  // replica_start + per MD step (integrate, force: lists + pairs in FP32, one launch in FP64;
+  // with velocity scaling also the rescale and, after the first step, the closing kick)
   // + replica_end + the device exchange when enabled
   if (!h) return 0;
-  return (h->prec == kF32 ? 3 : 2) * h->interval + 2 + (h->exch_enabled ? 1 : 0);
+  const int per_step = (h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0);
+  return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0);
 }
 
 long long remd_replica_pair_count(remd_handle h, int rep) {
@@ -827,7 +855,7 @@ remd_status remd_profile_steps(remd_handle h, int nsteps, double* ms_out) {
   double ti = 0.0, tf = 0.0;
   for (int s = 0; s < nsteps; s++) {
     CK(cudaEventRecord(ev[0], h->stream));
-    launch_integrate_prec(h->d, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+    launch_step_integrate(h, s);
     CK(cudaEventRecord(ev[1], h->stream));
     launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
     CK(cudaEventRecord(ev[2], h->stream));

@@ -1162,10 +1162,43 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_props(DevPtrs d, RepSta
   }
 }
 
-// Molecules::KillMomentum + KillAngularMomentumInTube (src/molecules.cxx:168-210)
-// for the replica of this block; L and s from st.
+// Molecules::KillAngularMomentumInTube (src/molecules.cxx:189-210) for the
+// replica of this block: the mean angular momentum about the tube axis, taken
+// out of molecules further than 1 A from it; L and s from st.
+__device__ void kill_tube_angular_block(const DevPtrs& d, const RepConst& c, const RepState& st,
+                                        double* red) {
+  const int N = d.N;
+  double am[4] = {0, 0, 0, 0};
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    double r[3], v[3];
+    for (int x = 0; x < 3; x++) {
+      r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+      v[x] = d.v[x * N + g] / (st.L[x] * st.s);
+    }
+    am[0] += c.mass * (r[0] * v[1] - r[1] * v[0]);
+    am[1] += c.mass;
+  }
+  block_sum<4>(am, red);
+  const double lz = am[0] / am[1];
+  for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
+    const int g = c.mol_off + li;
+    double r[3];
+    for (int x = 0; x < 3; x++) r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
+    const double r02 = r[0] * r[0] + r[1] * r[1];
+    if (r02 > 1.0) {
+      d.v[g] += lz * r[1] / r02 * st.L[0] * st.s;
+      d.v[N + g] -= lz * r[0] / r02 * st.L[1] * st.s;
+    }
+  }
+  __syncthreads();
+}
+
+// Molecules::KillMomentum (src/molecules.cxx:168-187) for the replica of this
+// block: the mean momentum removed along the unconfined directions; in a tube
+// (z only) it also removes the angular momentum about the axis.
 __device__ void kill_momentum_block(const DevPtrs& d, const RepConst& c, const RepState& st,
-                                    double* red, bool tube_angular) {
+                                    double* red) {
   const int N = d.N;
   double acc[4] = {0, 0, 0, 0};
   for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
@@ -1187,32 +1220,7 @@ __device__ void kill_momentum_block(const DevPtrs& d, const RepConst& c, const R
     }
   }
   __syncthreads();
-  if (c.confined == 1 && tube_angular) {
-    double am[4] = {0, 0, 0, 0};
-    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
-      const int g = c.mol_off + li;
-      double r[3], v[3];
-      for (int x = 0; x < 3; x++) {
-        r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
-        v[x] = d.v[x * N + g] / (st.L[x] * st.s);
-      }
-      am[0] += c.mass * (r[0] * v[1] - r[1] * v[0]);
-      am[1] += c.mass;
-    }
-    block_sum<4>(am, red);
-    const double lz = am[0] / am[1];
-    for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
-      const int g = c.mol_off + li;
-      double r[3];
-      for (int x = 0; x < 3; x++) r[x] = (d.r[x * N + g] - 0.5) * st.L[x];
-      const double r02 = r[0] * r[0] + r[1] * r[1];
-      if (r02 > 1.0) {
-        d.v[g] += lz * r[1] / r02 * st.L[0] * st.s;
-        d.v[N + g] -= lz * r[0] / r02 * st.L[1] * st.s;
-      }
-    }
-    __syncthreads();
-  }
+  if (c.confined == 1) kill_tube_angular_block(d, c, st, red);
 }
 
 // The exchange tail for a replica whose condition changed (src/remd.cxx:526-536):
@@ -1251,7 +1259,7 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
     for (int x = 0; x < 4; x++) d.p[x * N + g] *= sc;
   }
   __syncthreads();
-  kill_momentum_block(d, c, st, red, true);
+  kill_momentum_block(d, c, st, red);
   double kacc[4];
   kinetic_sums(d, c, st.s, kacc);
   block_sum<4>(kacc, red);
@@ -1263,22 +1271,30 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
   }
 }
 
-// Molecules::VelocityScaling + AngVelocityScaling (src/molecules.cxx:262-307), the
-// reference's init_scaling: translational and rotational kinetic energies set to
-// 1.5 N T each, momentum removed, thermostat and barostat momenta reset, then H0
-// recomputed (InitializeProperty).  The stored v and p carry a factor s; they
-// are first brought to s = 1 (the reference calls this only at start-up, where
-// s = 1 already, and resetting s afterwards would otherwise scale the kinetic
-// energy by 1/s^2).
+// Molecules::VelocityScaling + AngVelocityScaling (src/molecules.cxx:261-311):
+// translational and rotational kinetic energies set to 1.5 N T each, momentum
+// removed (along z plus the angular momentum about the axis in a tube),
+// thermostat and barostat momenta reset.
+//  PER_STEP = false: the reference's init_scaling, after which H0 is recomputed
+//    (InitializeProperty).  The stored v and p carry a factor s; they are first
+//    brought to s = 1 (the reference calls this only at start-up, where s = 1
+//    already, and resetting s afterwards would otherwise scale the kinetic
+//    energy by 1/s^2).
+//  PER_STEP = true: the velocity-scaling thermostat (tconstant 2) before every
+//    MD step, for those replicas only, in the reference's exact order (kinetic
+//    energy with the current s, then s = 1, then the rotational part); H0 and
+//    the averages are left alone.
+template <bool PER_STEP>
 __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepState* X) {
   __shared__ RepState st;
   __shared__ double red[8 * 4];
   const int rep = blockIdx.x;
   const RepConst& c = d.rc[rep];
+  if (PER_STEP && c.tconstant != 2) return;   // uniform for the block
   if (threadIdx.x == 0) st = X[rep];
   __syncthreads();
   const int N = d.N;
-  if (st.s != 1.0) {
+  if (!PER_STEP && st.s != 1.0) {
     const double si = 1.0 / st.s;
     for (int li = threadIdx.x; li < c.nmol; li += blockDim.x) {
       const int g = c.mol_off + li;
@@ -1303,8 +1319,9 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepS
       for (int x = 0; x < 3; x++) d.v[x * N + c.mol_off + li] *= coef;
   }
   __syncthreads();
-  kill_momentum_block(d, c, st, red, true);
-  if (c.confined == 1) kill_momentum_block(d, c, st, red, true);
+  kill_momentum_block(d, c, st, red);
+  // VelocityScaling takes the tube's angular momentum out once more after KillMomentum
+  if (c.confined == 1) kill_tube_angular_block(d, c, st, red);
   __syncthreads();
   if (threadIdx.x == 0) {
     st.s = 1.0;
@@ -1320,6 +1337,10 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepS
       for (int x = 0; x < 4; x++) d.p[x * N + c.mol_off + li] *= coef;
   }
   __syncthreads();
+  if (PER_STEP) {
+    if (threadIdx.x == 0) X[rep] = st;
+    return;
+  }
   kinetic_sums(d, c, st.s, k);
   block_sum<4>(k, red);
   if (threadIdx.x == 0) {
@@ -1556,8 +1577,9 @@ void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s) {
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s) {
   k_replica_props<<<d.nrep, kRepThreads, 0, s>>>(d, X);
 }
-void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s) {
-  k_replica_rescale<<<d.nrep, kRepThreads, 0, s>>>(d, X);
+void launch_replica_rescale(const DevPtrs& d, RepState* X, bool per_step, cudaStream_t s) {
+  if (per_step) k_replica_rescale<true><<<d.nrep, kRepThreads, 0, s>>>(d, X);
+  else k_replica_rescale<false><<<d.nrep, kRepThreads, 0, s>>>(d, X);
 }
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, const unsigned long long* seeds,

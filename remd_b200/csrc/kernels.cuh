@@ -34,7 +34,7 @@ void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int pre
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);
-void launch_replica_rescale(const DevPtrs& d, RepState* X, cudaStream_t s);
+void launch_replica_rescale(const DevPtrs& d, RepState* X, bool per_step, cudaStream_t s);
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, const unsigned long long* seeds,
                        int* index, double* T, double* P, long long* step_ctr, cudaStream_t s);

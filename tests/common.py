@@ -15,6 +15,8 @@ CASES = {
     "tip4p_bulk_nve": ("tip4p", 0, 0, 0, 64, 104),
     "tip5p_tube_nvt": ("tip5p", 1, 0, 1, 80, 105),
     "tip3p_tube_npz": ("tip3p", 1, 2, 1, 72, 106),
+    "tip4p_bulk_vscale": ("tip4p", 0, 0, 2, 64, 107),
+    "tip3p_tube_npz_vscale": ("tip3p", 1, 2, 2, 72, 108),
 }
 NSTEPS = 20
 

@@ -3,7 +3,7 @@
 Run in a container that has the reference sources (it builds oracle/_ref from
 them with oracle/Makefile):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]     (all cases when none is named)
 
 Writes, next to this script:
   gpu0000.chk          copy of the reference's test input (test/input/gpu0000.chk)
@@ -38,6 +38,8 @@ CASES = {
     "tip4p_bulk_nve": ("tip4p", 0, 0, 0, 64, 104),
     "tip5p_tube_nvt": ("tip5p", 1, 0, 1, 80, 105),
     "tip3p_tube_npz": ("tip3p", 1, 2, 1, 72, 106),
+    "tip4p_bulk_vscale": ("tip4p", 0, 0, 2, 64, 107),
+    "tip3p_tube_npz_vscale": ("tip3p", 1, 2, 2, 72, 108),
 }
 NSTEPS = 20
 
@@ -67,7 +69,7 @@ def main():
     json.dump({"source": "test/correct:4", "columns": cols,
                "values": [float(x) for x in line[3:]]},
               open(os.path.join(HERE, "correct_line.json"), "w"), indent=1)
-    for name in CASES:
+    for name in (sys.argv[1:] or CASES):
         ens = case_ensemble(name)
         spec, st = ens.spec, ens.states[0]
         ref = O.Reference(spec, st, spec.moltype_file)

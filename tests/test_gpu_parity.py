@@ -154,6 +154,55 @@ def test_batch_equals_alone_bitwise():
             k += 1
 
 
+def test_velocity_scaling_in_a_mixed_batch():
+    """tconstant 2: Molecules::ExecuteSteps rescales the velocities before every
+    step (src/integrator.cxx:713-723).  In a batch with Nose-Poincare replicas the
+    scaled replicas follow the oracle, and the others stay bit-identical to a
+    batch without them (their steps are split into closing kick, rescale
+    launch and opening, with the same arithmetic as the fused step)."""
+    vs = S.small_ensemble("tip3p", 1, nmol=72, ntemp=2, npress=1, seed=51, interval=NSTEPS,
+                          pconstant=2, tconstant=2)
+    npt = S.small_ensemble("tip4p", 0, nmol=70, ntemp=2, npress=1, seed=52, interval=NSTEPS)
+    for prec in ["fp32", "fp64"]:
+        mixed = E.REMDGPU([npt, vs], precision=prec)
+        plain = E.REMDGPU([npt], precision=prec)
+        assert mixed.launches_per_interval() == plain.launches_per_interval() + 2 * NSTEPS - 1
+        T = np.concatenate([npt.T, vs.T])
+        P = np.concatenate([npt.P, vs.P])
+        mixed.ExecuteSteps(T, P)
+        plain.ExecuteSteps(npt.T, npt.P)
+        for j in range(2):
+            assert np.array_equal(mixed.GetAverages(j), plain.GetAverages(j))
+            assert np.array_equal(mixed.ConvertVariablesToHost(j)["v"], plain.ConvertVariablesToHost(j)["v"])
+        for j, st in enumerate(vs.states):
+            orc = O.Oracle(vs.spec, st)
+            orc.initialize_property()
+            orc.steps(NSTEPS)
+            a, b = mixed.GetAverages(2 + j), orc.average()
+            g = mixed.ConvertVariablesToHost(2 + j)
+            tr, te = (1e-9, 1e-8) if prec == "fp64" else (2e-5, 2e-4)
+            assert rel(g["r"], orc.r) < tr
+            assert a[0] + a[1] + a[2] == pytest.approx(b[0] + b[1] + b[2], rel=te)
+            for k in [3, 4, 5, 6]:   # VOL TRA ROT T
+                assert a[k] == pytest.approx(b[k], rel=te * 10), E.AVG_NAMES[k]
+            # s and Ps are reset before every step and not integrated; Pv_z restarts from 0
+            assert a[13] == 1.0 and a[14] == 0.0
+            assert a[17] == pytest.approx(b[17], rel=te * 10, abs=1e-12)
+        mixed.close()
+        plain.close()
+
+
+def test_velocity_scaling_modes_the_reference_does_not_integrate_are_rejected():
+    """Slit and bulk-barostat *TSCALE* modes fall through the switch of
+    Molecules::ExecuteSteps (src/integrator.cxx:730-787), which then integrates
+    nothing; the engine refuses them."""
+    for confined, pcon in [(2, 0), (2, 3), (0, 1)]:
+        e = S.small_ensemble("tip4p", confined, nmol=64, ntemp=1, npress=1, seed=53, interval=5,
+                             pconstant=pcon, tconstant=2)
+        with pytest.raises(RuntimeError, match="tconstant 2"):
+            E.REMDGPU([e], precision="fp32")
+
+
 def test_device_exchange_equals_host_exchange():
     ens = [S.small_ensemble("tip4p", 0, nmol=64, ntemp=4, npress=2, seed=41, interval=5),
            S.small_ensemble("tip3p", 1, nmol=80, ntemp=2, npress=3, seed=42, interval=5)]
