@@ -264,6 +264,12 @@ remd_status remd_write_chk(remd_handle h, int rep, const char *path);
  * MakeMolTypeList does (src/molecules.cxx:86, 95). */
 remd_status remd_write_gro(remd_handle h, int rep, const char *path, const char *mol_name,
                            const char *const *atom_names);
+/* REMDGPU::OutputCDV (src/remdgpu.cu:700-804): a CDView snapshot of every
+ * replica to <prefix>R%04d s%07d .cdv (rep, step): box (tube: +-wall_length in
+ * x, y; slit: +-wall_length/2 in z), colours, "T=.. K, P=.. MPa", then one line
+ * "mol site x y z" per site in A from the box centre, in the reference's single
+ * precision. */
+remd_status remd_output_cdv(remd_handle h, const char *prefix, unsigned int step);
 
 /* Force snapshot of one replica that allocates nothing.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory -- a host

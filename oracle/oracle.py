@@ -271,6 +271,51 @@ def gro_text(molid, molname, atomname, atomid, coor, L, comment="test"):
     return "\n".join(out) + "\n"
 
 
+def cdv_text(r, q, L, body, T, P, confined, wall_length):
+    """One replica's snapshot as REMDGPU::OutputCDV writes it (src/remdgpu.cu:700-804),
+    from its GPU state: the centre as the fixed-point box fraction (int)(2^32 (r-1/2))
+    (src/remdgpu.cu:261-263), box and wall length as float, site offsets from the
+    device M2A in double (src/remdgpu.cu:2607-2634, body coordinates as float) rounded
+    to float, each printed as float(centre) * float(L 2^-32) + offset.  T, P reduced,
+    held as float (cond0).  Numbers in the C++ stream default format (%g)."""
+    from remd_b200.inputs import UNIT_PRESS, UNIT_TEMP
+    f32 = np.float32
+    g = lambda x: "%g" % float(x)  # noqa: E731
+    Lf = np.asarray(L, dtype=f32)
+    wl = f32(wall_length)
+    lo = [-0.5 * float(Lf[d]) for d in range(3)]
+    hi = [0.5 * float(Lf[d]) for d in range(3)]
+    if confined == 1:
+        lo[0] = lo[1] = -float(wl)
+        hi[0] = hi[1] = float(wl)
+    elif confined == 2:
+        lo[2], hi[2] = -0.5 * float(wl), 0.5 * float(wl)
+    head = "'" + "".join(" box_s%s=%s" % (a, g(v)) for a, v in zip("xyz", lo))
+    head += "".join(" box_e%s=%s" % (a, g(v)) for a, v in zip("xyz", hi))
+    head += (" r0=1.0 r1=0.8 r2=0.8 c0=(1.0,0.0,0.0) c1=(1.0,1.0,1.0) c2=(1.0,1.0,1.0)"
+             " bond0_c=(1.0,1.0,1.0)")
+    Tk = float(f32(T)) * UNIT_TEMP
+    Pp = float(f32(P)) * UNIT_PRESS
+    head += ' st0="T=%s K, P=%s MPa" st0_pos=(-2.0,-2.0)' % (g(Tk), g(Pp / 1e6))
+    lines = [head]
+    itof = Lf * f32(2.0 ** -32)
+    b = np.asarray(body, dtype=f32).astype(float)
+    for i in range(len(r)):
+        gi = [int(4294967296.0 * (float(r[i][d]) - 0.5)) for d in range(3)]
+        x, y, z, w = (float(v) for v in q[i])
+        sx, sy, sz, sw = x * x, y * y, z * z, w * w
+        xy, xz, xw = 2 * x * y, 2 * x * z, 2 * x * w
+        yz, yw, zw = 2 * y * z, 2 * y * w, 2 * z * w
+        for k in range(len(b)):
+            bx, by, bz = b[k]
+            ar = ((sx + sy - sz - sw) * bx + (yz - xw) * by + (yw + xz) * bz,
+                  (yz + xw) * bx + (sx - sy + sz - sw) * by + (zw - xy) * bz,
+                  (yw - xz) * bx + (zw + xy) * by + (sx - sy - sz + sw) * bz)
+            pos = [f32(f32(gi[d]) * itof[d]) + f32(ar[d]) for d in range(3)]
+            lines.append("%d %d %s %s %s" % (i, k, g(pos[0]), g(pos[1]), g(pos[2])))
+    return "\n".join(lines) + "\n"
+
+
 def reference_write_gro(path, molid, molname, atomname, atomid, coor, L, comment="test"):
     """The reference's own write_gro_file (src/gro.cxx:118-135, compiled into
     oracle/_ref) on the same atoms."""

@@ -7,6 +7,9 @@
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -1020,6 +1023,75 @@ remd_status remd_write_gro(remd_handle h, int rep, const char* path, const char*
   if (!ok) {
     set_error(std::string("remd_write_gro: write failed: ") + path);
     return REMD_ERR_IO;
+  }
+  return REMD_OK;
+}
+
+// REMDGPU::OutputCDV (src/remdgpu.cu:700-804): one CDView snapshot per replica,
+// <prefix>R<rep, 4 digits>s<step, 7 digits>.cdv.  The numbers are the ones that
+// the reference's GPU state holds and prints: the centre of mass as a 32-bit
+// fixed-point box fraction (int)(2^32 (r - 1/2)), the box and the wall length
+// in single precision, the site offsets R(q) b rounded to float, each site
+// printed as float(centre * (L 2^-32)) + offset; the condition as the float it
+// keeps (cond0), in K and MPa.  Text formatting is the C++ stream default
+// (6 significant digits), as in the reference.
+remd_status remd_output_cdv(remd_handle h, const char* prefix, unsigned int step) {
+  if (!h || !prefix) return REMD_ERR_INVALID;
+  const float to_frac = (float)kFixInv;   // 2^-32, exact in float
+  for (int rep = 0; rep < h->nrep; rep++) {
+    const RepConst& c = h->rc[rep];
+    const int n = c.nmol, ns = c.nsite;
+    std::vector<double> r(3 * n), q(4 * n);
+    remd_state_view o;
+    std::memset(&o, 0, sizeof(o));
+    o.r = r.data(); o.q = q.data();
+    remd_status st = remd_get_state(h, rep, &o);
+    if (st != REMD_OK) return st;
+    std::ostringstream name;
+    name << prefix << "R" << std::setw(4) << std::setfill('0') << rep << "s" << std::setw(7)
+         << std::setfill('0') << step << ".cdv";
+    std::ofstream os(name.str());
+    if (!os) {
+      set_error("remd_output_cdv: cannot open " + name.str());
+      return REMD_ERR_IO;
+    }
+    const float L[3] = {(float)o.L[0], (float)o.L[1], (float)o.L[2]};
+    const float wl = (float)c.wall_length_param;
+    const float ItoF[3] = {L[0] * to_frac, L[1] * to_frac, L[2] * to_frac};
+    os << "'";
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; d++) { lo[d] = -0.5 * L[d]; hi[d] = 0.5 * L[d]; }
+    if (c.confined == 1) { lo[0] = lo[1] = -wl; hi[0] = hi[1] = wl; }
+    if (c.confined == 2) { lo[2] = -0.5 * wl; hi[2] = 0.5 * wl; }
+    os << " box_sx=" << lo[0] << " box_sy=" << lo[1] << " box_sz=" << lo[2];
+    os << " box_ex=" << hi[0] << " box_ey=" << hi[1] << " box_ez=" << hi[2];
+    // site radii and colours (oxygen red, the rest white) and the condition label
+    os << " r0=1.0 r1=0.8 r2=0.8 c0=(1.0,0.0,0.0) c1=(1.0,1.0,1.0) c2=(1.0,1.0,1.0)"
+          " bond0_c=(1.0,1.0,1.0)";
+    const double T = (double)(float)o.T * unit_temp(), P = (double)(float)o.P * unit_press();
+    os << " st0=\"T=" << T << " K, P=" << P / 1e6 << " MPa\" st0_pos=(-2.0,-2.0)\n";
+    for (int i = 0; i < n; i++) {
+      int g[3];
+      for (int d = 0; d < 3; d++) g[d] = (int)(kFix * (r[3 * i + d] - 0.5));
+      const double qi[4] = {q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+      for (int k = 0; k < ns; k++) {
+        const double b[3] = {(double)(float)c.body[k][0], (double)(float)c.body[k][1],
+                             (double)(float)c.body[k][2]};
+        double sk[3];
+        body_to_space(qi, b, sk);
+        os << i << " " << k;
+        for (int d = 0; d < 3; d++) {
+          const float a = (float)g[d] * ItoF[d] + (float)sk[d];
+          os << " " << a;
+        }
+        os << "\n";
+      }
+    }
+    os.close();
+    if (!os) {
+      set_error("remd_output_cdv: write failed: " + name.str());
+      return REMD_ERR_IO;
+    }
   }
   return REMD_OK;
 }

@@ -424,6 +424,11 @@ class REMDGPU:
     def write_chk(self, rep, path):
         _check(lib().remd_write_chk(self.h, rep, path.encode()))
 
+    def OutputCDV(self, prefix, step):
+        """REMDGPU::OutputCDV: a <prefix>R%04ds%07d.cdv snapshot of every replica
+        (remd_output_cdv)."""
+        _check(lib().remd_output_cdv(self.h, prefix.encode(), C.c_uint(step)))
+
     def write_gro(self, rep, path, moltype):
         """The reference's .gro output of replica rep (remd_write_gro); names from
         the molecule type."""

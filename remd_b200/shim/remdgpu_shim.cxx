@@ -148,24 +148,11 @@ void REMDGPU::OutputCheckPoint(const char* prefix, const int* index) {
   }
 }
 
-// .cdv snapshots (src/remdgpu.cu:700-804) are a visualisation aid, not part of the
-// engine: this writes the molecule centres only.
+// .cdv snapshots of every replica (src/remdgpu.cu:700-804); the reference writes
+// them per replica slot, not per condition, so index is not used there either.
 void REMDGPU::OutputCDV(const char* prefix, const unsigned int step, const int* index) {
-  std::vector<double> r(3 * nmol_);
-  for (unsigned rep = 0; rep < nreplica_; rep++) {
-    remd_state_view sv{};
-    sv.r = r.data();
-    check(remd_get_state(h_, (int)rep, &sv), "remd_get_state");
-    std::stringstream s;
-    s << prefix << "R" << std::setw(4) << std::setfill('0') << rep << "s" << std::setw(7) << step << ".cdv";
-    std::ofstream os(s.str());
-    os << "' box_sx=" << -0.5 * sv.L[0] << " box_sy=" << -0.5 * sv.L[1] << " box_sz=" << -0.5 * sv.L[2]
-       << " box_ex=" << 0.5 * sv.L[0] << " box_ey=" << 0.5 * sv.L[1] << " box_ez=" << 0.5 * sv.L[2] << "\n";
-    for (int i = 0; i < nmol_; i++)
-      os << i << " 0 " << (r[3 * i] - 0.5) * sv.L[0] << " " << (r[3 * i + 1] - 0.5) * sv.L[1] << " "
-         << (r[3 * i + 2] - 0.5) * sv.L[2] << "\n";
-  }
   (void)index;
+  check(remd_output_cdv(h_, prefix, step), "remd_output_cdv");
 }
 
 void REMDGPU::PrintAll(std::ostream& os) {

@@ -108,3 +108,7 @@ def test_reference_remd_driver_runs_on_the_engine(tmp_path):
     assert st.r.shape == (150, 3) and np.all((st.r >= 0) & (st.r <= 1))
     gro = open(out / "gpu0000.gro").read().splitlines()
     assert gro[0] == "test" and int(gro[1]) == 600 and len(gro) == 603
+    # .cdv snapshot of step 0 (snap_interval) through REMDGPU::OutputCDV
+    cdv = open(out / "gpuR0000s0000000.cdv").read().splitlines()
+    assert cdv[0].startswith("' box_sx=-7.4 box_sy=-7.4 ") and 'st0="T=200 K, P=4000 MPa"' in cdv[0]
+    assert len(cdv) == 601 and cdv[1].split()[:2] == ["0", "0"] and cdv[600].split()[:2] == ["149", "3"]

@@ -478,3 +478,28 @@ def test_write_gro_matches_reference_writer(tmp_path):
         O.reference_write_gro(ref, *atoms, L=g["L"] * 0.1)
         assert open(ref).read() == text
     eng.close()
+
+
+def test_output_cdv_matches_restatement(tmp_path):
+    """remd_output_cdv (REMDGPU::OutputCDV, src/remdgpu.cu:700-804) over a batch of
+    bulk, tube and slit replicas after an interval: one file per replica slot,
+    byte-identical to the restatement on the engine's own state."""
+    ens = [S.small_ensemble("tip3p", 0, nmol=70, ntemp=2, npress=1, seed=61, interval=10),
+           S.small_ensemble("tip4p", 1, nmol=96, ntemp=1, npress=2, seed=62, interval=10),
+           S.small_ensemble("tip5p", 2, nmol=80, ntemp=1, npress=1, seed=63, interval=10)]
+    eng = E.REMDGPU(ens, precision="fp32")
+    eng.ExecuteSteps(np.concatenate([e.T for e in ens]), np.concatenate([e.P for e in ens]))
+    prefix = str(tmp_path / "snap")
+    eng.OutputCDV(prefix, 12)
+    k = 0
+    for e in ens:
+        for _ in e.states:
+            g = eng.ConvertVariablesToHost(k)
+            want = O.cdv_text(g["r"], g["q"], g["L"], e.spec.moltype.r, g["T"], g["P"],
+                              e.spec.confined, e.spec.wall_length)
+            got = open(f"{prefix}R{k:04d}s0000012.cdv").read()
+            assert got == want, k
+            assert len(got.splitlines()) == 1 + e.spec.nmol * e.spec.moltype.nsite
+            k += 1
+    assert not os.path.exists(f"{prefix}R{k:04d}s0000012.cdv")
+    eng.close()

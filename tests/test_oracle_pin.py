@@ -114,3 +114,26 @@ def test_gro_restatement_matches_reference_writer(tmp_path):
     lines = text.splitlines()
     assert lines[0] == "test" and int(lines[1]) == 40 * 5 and len(lines) == 40 * 5 + 3
     assert lines[2][5:15] == "TIP5P   OW"
+
+
+def test_cdv_restatement_known_answer():
+    """REMDGPU::OutputCDV (src/remdgpu.cu:700-804), worked by hand for a tube box:
+    the box spans +-wall_length in x and y, the centres come from the 32-bit
+    fixed-point fraction (r = 0.1 of 30 A prints as -12 after the float
+    rounding), and the sites are offset by R(q) b."""
+    from remd_b200.inputs import UNIT_PRESS, UNIT_TEMP
+    r = np.array([[0.5, 0.5, 0.5], [0.25, 0.75, 0.1]])
+    q = np.array([[1.0, 0.0, 0.0, 0.0], [0.5, 0.5, 0.5, 0.5]])
+    text = O.cdv_text(r, q, [20.0, 20.0, 30.0], [[0.0, 0.0, 0.0], [0.75, 0.5, 0.0]], 2.5, 0.0625,
+                      confined=1, wall_length=6.0)
+    lines = text.splitlines()
+    assert lines[0] == ("' box_sx=-6 box_sy=-6 box_sz=-15 box_ex=6 box_ey=6 box_ez=15"
+                        " r0=1.0 r1=0.8 r2=0.8 c0=(1.0,0.0,0.0) c1=(1.0,1.0,1.0) c2=(1.0,1.0,1.0)"
+                        ' bond0_c=(1.0,1.0,1.0) st0="T=%g K, P=%g MPa" st0_pos=(-2.0,-2.0)'
+                        % (2.5 * UNIT_TEMP, 0.0625 * UNIT_PRESS / 1e6))
+    assert lines[1:] == ["0 0 0 0 0", "0 1 0.75 0.5 0", "1 0 -5 5 -12", "1 1 -5 5.75 -11.5"]
+    # bulk and slit boxes
+    bulk = O.cdv_text(r[:1], q[:1], [20.0, 20.0, 30.0], [[0.0, 0.0, 0.0]], 2.5, 0.0625, 0, 0.0)
+    assert bulk.startswith("' box_sx=-10 box_sy=-10 box_sz=-15 box_ex=10 box_ey=10 box_ez=15 ")
+    slit = O.cdv_text(r[:1], q[:1], [20.0, 20.0, 30.0], [[0.0, 0.0, 0.0]], 2.5, 0.0625, 2, 9.0)
+    assert slit.startswith("' box_sx=-10 box_sy=-10 box_sz=-4.5 box_ex=10 box_ey=10 box_ez=4.5 ")
