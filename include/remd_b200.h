@@ -41,7 +41,8 @@ typedef enum {
   REMD_ERR_CUDA = 6,           /* CUDA runtime error (message in remd_last_error)    */
   REMD_ERR_IO = 7,             /* file could not be read or written                  */
   REMD_ERR_NEIGHBOR_OVERFLOW = 8, /* a neighbour list exceeded its capacity          */
-  REMD_ERR_NO_DEVICE = 9       /* no CUDA device                                     */
+  REMD_ERR_NO_DEVICE = 9,      /* no CUDA device                                     */
+  REMD_ERR_RANGE = 10          /* a histogram sample fell outside its range          */
 } remd_status;
 
 #define REMD_NUM_AVERAGES 19   /* Average::NUM_ELEM, src/remdinfo.h:29-41 */
@@ -270,6 +271,32 @@ remd_status remd_write_gro(remd_handle h, int rep, const char *path, const char 
  * "mol site x y z" per site in A from the box centre, in the reference's single
  * precision. */
 remd_status remd_output_cdv(remd_handle h, const char *prefix, unsigned int step);
+
+/* ---- (volume, potential) histograms on the device ------------------------- */
+/* REMDInfo's per-condition histograms (src/remdinfo.h:93-139, 299-331; 500 x 500
+ * bins, linear sampling), kept on the device for ensemble ens: one per condition
+ * slot, with the 19 Average fields summed per bin.  energy in kJ/mol and volume
+ * in A^3, both per molecule (the .inp energy_min/max, volume_min/max).  Enabling
+ * again clears it.  About 39 MB of device memory per condition slot. */
+remd_status remd_histogram_enable(remd_handle h, int ens, double energy_min, double energy_max,
+                                  double volume_min, double volume_max);
+/* REMD::IncrementHistogram (src/remd.cxx:803-813) after an interval: the slot c
+ * histogram of each ensemble gets the sample of the replica index[c] holds
+ * (ensemble-local indices, ensembles concatenated like the replicas).  index
+ * NULL: the engine's own index (the device exchange's).  With the device
+ * exchange enabled the interval graph already does this before exchanging; do
+ * not call it then.  A sample out of range returns REMD_ERR_RANGE (the
+ * reference exits). */
+remd_status remd_histogram_increment(remd_handle h, const int *index);
+/* One slot's histogram: bounds = {vmin, vmax, pmin, pmax, samples}, hist the
+ * 500 x 500 counts (volume-major), ave the 500 x 500 x 19 per-bin sums; any may
+ * be NULL. */
+remd_status remd_histogram_get(remd_handle h, int ens, int slot, int *bounds, int *hist, double *ave);
+/* REMDInfo::OutputHistogram (src/remdinfo.cxx:723-758): dir/histo_P%lf_T%lf.dat
+ * per slot, with the slot's reduced condition. */
+remd_status remd_histogram_write(remd_handle h, int ens, const char *dir);
+/* REMDInfo::ReadHistogramFromBackUp (src/remdinfo.cxx:681-721) from those files. */
+remd_status remd_histogram_read(remd_handle h, int ens, const char *dir);
 
 /* Force snapshot of one replica that allocates nothing.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory -- a host

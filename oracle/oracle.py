@@ -316,6 +316,59 @@ def cdv_text(r, q, L, body, T, P, confined, wall_length):
     return "\n".join(lines) + "\n"
 
 
+class Histograms:
+    """REMDInfo's (volume, potential) histograms, one per condition slot
+    (src/remdinfo.h:93-139, 299-331; 500 x 500 bins, linear sampling), fed as
+    REMD::IncrementHistogram feeds them (src/remd.cxx:803-813) and written as
+    REMDInfo::OutputHistogram writes them (src/remdinfo.cxx:723-758)."""
+    NB = 500
+
+    def __init__(self, nslot, energy_min, energy_max, volume_min, volume_max):
+        self.emin, self.emax, self.vmin, self.vmax = energy_min, energy_max, volume_min, volume_max
+        self.de = (energy_max - energy_min) / float(self.NB)
+        self.dv = (volume_max - volume_min) / float(self.NB)
+        self.hist = np.zeros((nslot, self.NB, self.NB), dtype=np.int64)
+        self.ave = np.zeros((nslot, self.NB, self.NB, 19))
+        self.bounds = np.zeros((nslot, 5), dtype=np.int64)   # vmin vmax pmin pmax samples
+
+    def increment(self, index, avg, nmol):
+        """index[slot] = replica at that condition; avg (nrep, 19) GetAverages rows."""
+        for c, ind in enumerate(index):
+            a = avg[ind]
+            pot = (a[0] + a[1] + a[2]) / float(nmol)
+            vol = a[3] / float(nmol)
+            if vol < self.vmin or vol >= self.vmax or pot < self.emin or pot >= self.emax:
+                raise ValueError("potential energy or volume is not in the histogram range")
+            v = int((vol - self.vmin) / self.dv)
+            p = int((pot - self.emin) / self.de)
+            b = self.bounds[c]
+            if b[4] == 0:
+                b[0] = b[1] = v
+                b[2] = b[3] = p
+            b[0], b[1] = min(b[0], v), max(b[1], v)
+            b[2], b[3] = min(b[2], p), max(b[3], p)
+            b[4] += 1
+            self.hist[c, v, p] += 1
+            self.ave[c, v, p] += a
+
+    def text(self, c):
+        b = self.bounds[c]
+        out = ["#vmax vmin pmax pmin", "# %d %d %d %d" % (b[1], b[0], b[3], b[2])]
+        for v in range(b[0], b[1] + 1):
+            vol = self.vmin + v * self.dv
+            for p in range(b[2], b[3] + 1):
+                pot = self.emin + p * self.de
+                n = int(self.hist[c, v, p])
+                avg = self.ave[c, v, p] / n if n > 0 else np.zeros(19)
+                out.append(" %10.6e %10.6e %10d" % (vol, pot, n) + "".join(" %10.6e" % x for x in avg))
+            out.append("")
+        return "\n".join(out) + "\n"
+
+    @staticmethod
+    def file_name(directory, P, T):
+        return "%s/histo_P%f_T%f.dat" % (directory, P, T)
+
+
 def reference_write_gro(path, molid, molname, atomname, atomid, coor, L, comment="test"):
     """The reference's own write_gro_file (src/gro.cxx:118-135, compiled into
     oracle/_ref) on the same atoms."""
@@ -359,6 +412,10 @@ def _ref_lib(variant="generic"):
         lib.ref_remdinfo_exchange.restype = C.c_int
         lib.ref_remdinfo_exchange.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _ip]
         lib.ref_remdinfo_arrays.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        lib.ref_remdinfo_set_arrays.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        lib.ref_remdinfo_increment_histogram.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        lib.ref_remdinfo_output_histogram.argtypes = [C.c_void_p]
+        lib.ref_remdinfo_read_histogram.argtypes = [C.c_void_p]
         lib.ref_write_gro.argtypes = [C.c_char_p, C.c_int, _ip, C.POINTER(C.c_char_p),
                                       C.POINTER(C.c_char_p), _ip, _dp, _dp, C.c_char_p]
         for fn in ["ref_set_state", "ref_get_state", "ref_get_property", "ref_get_average",

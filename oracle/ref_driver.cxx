@@ -212,6 +212,34 @@ int ref_remdinfo_exchange(void* h, long step, const double* pot, const double* v
   return len;
 }
 
+// ---- (volume, potential) histograms of the compiled REMDInfo ----
+// Conditions and the condition-slot -> replica index, set from outside (the
+// exchange that moves them is pinned separately).
+void ref_remdinfo_set_arrays(void* h, const int* index, const double* T, const double* P) {
+  REMDInfo* ri = static_cast<REMDInfo*>(h);
+  for (int i = 0; i < ri->GetNumReplica(); i++) {
+    ri->index[i] = index[i];
+    ri->temperature[i] = T[i];
+    ri->pressure[i] = P[i];
+  }
+}
+// REMD::IncrementHistogram (src/remd.cxx:803-813) restated around the compiled
+// REMDInfo::IncrementHistogram / KeepAverages; ave = 19 Average fields per replica.
+void ref_remdinfo_increment_histogram(void* h, const double* pot, const double* vol, const double* ave) {
+  REMDInfo* ri = static_cast<REMDInfo*>(h);
+  for (int i = 0; i < ri->GetNumReplica(); ++i) {
+    const int ind = ri->GetIndex(i);
+    const double p = pot[ind] / (double)ri->GetNmol();
+    const double v = vol[ind] / (double)ri->GetNmol();
+    ri->IncrementHistogram(v, p, i);
+    Average a;
+    for (int k = 0; k < Average::NUM_ELEM; k++) a.sum[k] = ave[ind * Average::NUM_ELEM + k];
+    ri->KeepAverages(v, p, i, a);
+  }
+}
+void ref_remdinfo_output_histogram(void* h) { static_cast<REMDInfo*>(h)->OutputHistogram(); }
+void ref_remdinfo_read_histogram(void* h) { static_cast<REMDInfo*>(h)->ReadHistogramFromBackUp(); }
+
 // The reference's .gro writer (src/gro.cxx:118-135) on atoms given as arrays:
 // molecule id, molecule name, atom name, atom id, coordinates (nm); velocities 0.
 void ref_write_gro(const char* path, int natom, const int* molid, const char* const* molname,

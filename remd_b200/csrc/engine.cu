@@ -64,6 +64,13 @@ struct remd_engine_s {
   unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
   long long last_pairs = 0;
   size_t bytes = 0;
+  // (volume, potential) histograms per condition slot, per ensemble (own allocations)
+  std::vector<HistEns> hist;        // host copy of d_hist (device pointers inside)
+  HistEns* d_hist = nullptr;
+  int* d_hidx = nullptr;            // slot -> replica index of the last host increment
+  std::vector<int> h_hidx;
+  bool hist_on = false;             // some ensemble keeps a histogram
+  bool graph_hist = false;
 };
 
 static int valid_model(const remd_system_desc& s, int* c0) {
@@ -270,6 +277,10 @@ static remd_status sync_and_check(remd_engine_s* h) {
     set_error("a replica produced a non-finite energy (see remd_replica_status)");
     return REMD_ERR_NONFINITE;
   }
+  if (err & kErrHistRange) {
+    set_error("potential energy or volume is not in the histogram range");
+    return REMD_ERR_RANGE;
+  }
   return REMD_OK;
 }
 
@@ -320,6 +331,10 @@ static remd_status build_graph(remd_engine_s* h) {
     launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
   }
   launch_replica_end(h->d, h->X, h->stream);
+  // the histogram samples the interval before the exchange moves the conditions
+  // (REMD::ExecuteREMD: IncrementHistogram, then ReplicaExchange, src/remd.cxx:396-401)
+  if (h->exch_enabled && h->hist_on)
+    launch_histogram(h->d, h->d_hist, h->d_rep_off, h->d_index, h->stream);
   if (h->exch_enabled)
     launch_exchange_k(h->d, h->d_grid, h->d_rep_off, h->d_u_off, h->nens, -1, nullptr, h->d_seed,
                       h->d_index, h->dT, h->dP, h->d_step, h->stream);
@@ -337,6 +352,7 @@ static remd_status build_graph(remd_engine_s* h) {
   }
   h->graph_tile = h->tile;
   h->graph_exchange = h->exch_enabled;
+  h->graph_hist = h->hist_on;
   return REMD_OK;
 }
 
@@ -593,6 +609,13 @@ remd_status remd_destroy(remd_handle h) {
   if (h->hT) cudaFreeHost(h->hT);
   if (h->hP) cudaFreeHost(h->hP);
   if (h->havg) cudaFreeHost(h->havg);
+  for (auto& H : h->hist) {
+    if (H.hist) cudaFree(H.hist);
+    if (H.ave) cudaFree(H.ave);
+    if (H.bounds) cudaFree(H.bounds);
+  }
+  if (h->d_hist) cudaFree(h->d_hist);
+  if (h->d_hidx) cudaFree(h->d_hidx);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return REMD_OK;
@@ -711,7 +734,8 @@ remd_status remd_execute_steps_async(remd_handle h, const double* T, const doubl
     CK(cudaMemcpyAsync(h->dT, h->hT, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->dP, h->hP, h->nrep * 8, cudaMemcpyHostToDevice, h->stream));
   }
-  if (!h->gexec || h->graph_tile != h->tile || h->graph_exchange != h->exch_enabled) {
+  if (!h->gexec || h->graph_tile != h->tile || h->graph_exchange != h->exch_enabled ||
+      h->graph_hist != h->hist_on) {
     remd_status s = build_graph(h);
     if (s != REMD_OK) return s;
   }
@@ -831,10 +855,11 @@ long long remd_last_pair_count(remd_handle h) {
 int remd_launches_per_interval(remd_handle h) {
   // replica_start + per MD step (integrate, force: lists + pairs in FP32, one launch in FP64;
   // with velocity scaling also the rescale and, after the first step, the closing kick)
-  // + replica_end + the device exchange when enabled
+  // + replica_end + the device exchange when enabled (and the histogram before it)
   if (!h) return 0;
   const int per_step = (h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0);
-  return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0);
+  return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0) +
+         (h->exch_enabled && h->hist_on ? 1 : 0);
 }
 
 long long remd_replica_pair_count(remd_handle h, int rep) {
@@ -1092,6 +1117,204 @@ remd_status remd_output_cdv(remd_handle h, const char* prefix, unsigned int step
       set_error("remd_output_cdv: write failed: " + name.str());
       return REMD_ERR_IO;
     }
+  }
+  return REMD_OK;
+}
+
+// ---- histograms (REMDInfo's Histogram, src/remdinfo.h:93-139, 299-331) ----
+
+remd_status remd_histogram_enable(remd_handle h, int ens, double energy_min, double energy_max,
+                                  double volume_min, double volume_max) {
+  if (!h || ens < 0 || ens >= h->nens || !(energy_max > energy_min) || !(volume_max > volume_min)) {
+    set_error("remd_histogram_enable: need a valid ensemble and max > min");
+    return REMD_ERR_INVALID;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (!h->d_hist) {
+    CK(cudaMalloc(&h->d_hist, sizeof(HistEns) * h->nens));
+    CK(cudaMalloc(&h->d_hidx, sizeof(int) * h->nrep));
+    h->hist.assign(h->nens, HistEns{});
+    h->h_hidx.resize(h->nrep);
+    for (int e = 0; e < h->nens; e++)
+      for (int c = 0; c < h->ens_nrep[e]; c++) h->h_hidx[h->ens_rep_off[e] + c] = c;
+  }
+  HistEns& H = h->hist[ens];
+  if (H.hist) { cudaFree(H.hist); cudaFree(H.ave); cudaFree(H.bounds); H = HistEns{}; }
+  const size_t nc = (size_t)h->ens_nrep[ens];
+  const size_t bins = nc * kHistBins * kHistBins;
+  if (cudaMalloc(&H.hist, bins * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&H.ave, bins * kNumAvg * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&H.bounds, nc * 5 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    if (H.hist) cudaFree(H.hist);
+    if (H.ave) cudaFree(H.ave);
+    if (H.bounds) cudaFree(H.bounds);
+    H = HistEns{};
+    set_error("remd_histogram_enable: device allocation failed");
+    return REMD_ERR_OOM;
+  }
+  CK(cudaMemset(H.hist, 0, bins * sizeof(int)));
+  CK(cudaMemset(H.ave, 0, bins * kNumAvg * sizeof(double)));
+  CK(cudaMemset(H.bounds, 0, nc * 5 * sizeof(int)));
+  // REMDInfo::REMDInfo, linear sampling (src/remdinfo.cxx:180-186)
+  H.emin = energy_min; H.emax = energy_max; H.de = (energy_max - energy_min) / (double)kHistBins;
+  H.vmin = volume_min; H.vmax = volume_max; H.dv = (volume_max - volume_min) / (double)kHistBins;
+  CK(cudaMemcpy(h->d_hist, h->hist.data(), sizeof(HistEns) * h->nens, cudaMemcpyHostToDevice));
+  h->hist_on = true;
+  return REMD_OK;
+}
+
+remd_status remd_histogram_increment(remd_handle h, const int* index) {
+  if (!h || !h->hist_on) { set_error("remd_histogram_increment: no histogram enabled"); return REMD_ERR_INVALID; }
+  const int* d_idx = h->d_index;
+  if (index) {
+    for (int e = 0; e < h->nens; e++)
+      for (int c = 0; c < h->ens_nrep[e]; c++) {
+        const int k = index[h->ens_rep_off[e] + c];
+        if (k < 0 || k >= h->ens_nrep[e]) { set_error("remd_histogram_increment: index out of range"); return REMD_ERR_INVALID; }
+      }
+    std::copy(index, index + h->nrep, h->h_hidx.begin());
+    CK(cudaMemcpyAsync(h->d_hidx, h->h_hidx.data(), h->nrep * 4, cudaMemcpyHostToDevice, h->stream));
+    d_idx = h->d_hidx;
+  }
+  launch_histogram(h->d, h->d_hist, h->d_rep_off, d_idx, h->stream);
+  CK(cudaGetLastError());
+  return sync_and_check(h);
+}
+
+remd_status remd_histogram_get(remd_handle h, int ens, int slot, int* bounds, int* hist, double* ave) {
+  if (!h || ens < 0 || ens >= h->nens || !h->hist_on || !h->hist[ens].hist || slot < 0 ||
+      slot >= h->ens_nrep[ens]) {
+    set_error("remd_histogram_get: no such histogram");
+    return REMD_ERR_INVALID;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  const HistEns& H = h->hist[ens];
+  const size_t nb = (size_t)kHistBins * kHistBins;
+  if (bounds) CK(cudaMemcpy(bounds, H.bounds + 5 * slot, 5 * sizeof(int), cudaMemcpyDeviceToHost));
+  if (hist) CK(cudaMemcpy(hist, H.hist + nb * slot, nb * sizeof(int), cudaMemcpyDeviceToHost));
+  if (ave) CK(cudaMemcpy(ave, H.ave + nb * kNumAvg * slot, nb * kNumAvg * sizeof(double), cudaMemcpyDeviceToHost));
+  return REMD_OK;
+}
+
+// The condition of each slot of ensemble e as REMDInfo holds it
+// (temperature[index[slot]], pressure[index[slot]]).
+static remd_status slot_conditions(remd_engine_s* h, int e, std::vector<double>& Tc, std::vector<double>& Pc) {
+  std::vector<int> idx(h->nrep);
+  std::vector<double> T(h->nrep), P(h->nrep);
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->exch_enabled) {
+    CK(cudaMemcpy(idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(T.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(P.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
+  } else {
+    idx = h->h_hidx;
+    T = h->curT;
+    P = h->curP;
+  }
+  const int off = h->ens_rep_off[e], n = h->ens_nrep[e];
+  Tc.resize(n);
+  Pc.resize(n);
+  for (int c = 0; c < n; c++) {
+    Tc[c] = T[off + idx[off + c]];
+    Pc[c] = P[off + idx[off + c]];
+  }
+  return REMD_OK;
+}
+
+static std::string histo_name(const char* dir, double P, double T) {
+  char buf[1024];
+  std::snprintf(buf, sizeof(buf), "%s/histo_P%lf_T%lf.dat", dir, P, T);
+  return buf;
+}
+
+// REMDInfo::OutputHistogram (src/remdinfo.cxx:723-758), linear sampling.
+remd_status remd_histogram_write(remd_handle h, int ens, const char* dir) {
+  if (!h || !dir || ens < 0 || ens >= h->nens || !h->hist_on || !h->hist[ens].hist) {
+    set_error("remd_histogram_write: no such histogram");
+    return REMD_ERR_INVALID;
+  }
+  std::vector<double> Tc, Pc;
+  remd_status st = slot_conditions(h, ens, Tc, Pc);
+  if (st != REMD_OK) return st;
+  const HistEns& H = h->hist[ens];
+  const size_t nb = (size_t)kHistBins * kHistBins;
+  std::vector<int> hist(nb);
+  std::vector<double> ave(nb * kNumAvg);
+  for (int c = 0; c < h->ens_nrep[ens]; c++) {
+    int b[5];
+    st = remd_histogram_get(h, ens, c, b, hist.data(), ave.data());
+    if (st != REMD_OK) return st;
+    const std::string path = histo_name(dir, Pc[c], Tc[c]);
+    FILE* fp = std::fopen(path.c_str(), "w");
+    if (!fp) { set_error("remd_histogram_write: cannot open " + path); return REMD_ERR_IO; }
+    std::fprintf(fp, "#vmax vmin pmax pmin\n");
+    std::fprintf(fp, "# %d %d %d %d\n", b[1], b[0], b[3], b[2]);
+    for (int v = b[0]; v <= b[1]; v++) {
+      const double vol = H.vmin + v * H.dv;
+      for (int p = b[2]; p <= b[3]; p++) {
+        const double pot = H.emin + p * H.de;
+        const size_t bin = (size_t)v * kHistBins + p;
+        const int n = hist[bin];
+        std::fprintf(fp, " %10.6e %10.6e %10d", vol, pot, n);
+        for (int x = 0; x < kNumAvg; x++)   // Histogram::GetAverages: sum / count, 0 if empty
+          std::fprintf(fp, " %10.6e", n > 0 ? ave[bin * kNumAvg + x] / (double)n : 0.0);
+        std::fprintf(fp, "\n");
+      }
+      std::fprintf(fp, "\n");
+    }
+    if (std::fclose(fp) != 0) { set_error("remd_histogram_write: write failed: " + path); return REMD_ERR_IO; }
+  }
+  return REMD_OK;
+}
+
+// REMDInfo::ReadHistogramFromBackUp (src/remdinfo.cxx:681-721): counts and the
+// per-bin averages (times the count) of every slot, from the files
+// remd_histogram_write (OutputHistogram) made.
+remd_status remd_histogram_read(remd_handle h, int ens, const char* dir) {
+  if (!h || !dir || ens < 0 || ens >= h->nens || !h->hist_on || !h->hist[ens].hist) {
+    set_error("remd_histogram_read: no such histogram");
+    return REMD_ERR_INVALID;
+  }
+  std::vector<double> Tc, Pc;
+  remd_status st = slot_conditions(h, ens, Tc, Pc);
+  if (st != REMD_OK) return st;
+  const HistEns& H = h->hist[ens];
+  const size_t nb = (size_t)kHistBins * kHistBins;
+  std::vector<int> hist(nb);
+  std::vector<double> ave(nb * kNumAvg);
+  for (int c = 0; c < h->ens_nrep[ens]; c++) {
+    const std::string path = histo_name(dir, Pc[c], Tc[c]);
+    std::ifstream is(path);
+    if (!is) { set_error("remd_histogram_read: input histogram file " + path + " is not found"); return REMD_ERR_IO; }
+    std::string dummy;
+    int b[5] = {0, 0, 0, 0, 0};
+    is >> dummy >> dummy >> dummy >> dummy;
+    is >> dummy >> b[1] >> b[0] >> b[3] >> b[2];
+    if (!is || b[0] < 0 || b[1] >= kHistBins || b[2] < 0 || b[3] >= kHistBins || b[0] > b[1] || b[2] > b[3]) {
+      set_error("remd_histogram_read: bad header in " + path);
+      return REMD_ERR_IO;
+    }
+    std::fill(hist.begin(), hist.end(), 0);
+    std::fill(ave.begin(), ave.end(), 0.0);
+    for (int v = b[0]; v <= b[1]; v++)
+      for (int p = b[2]; p <= b[3]; p++) {
+        const size_t bin = (size_t)v * kHistBins + p;
+        int n = 0;
+        is >> dummy >> dummy >> n;
+        hist[bin] = n;
+        b[4] += n;
+        for (int x = 0; x < kNumAvg; x++) {
+          double a = 0.0;
+          is >> a;
+          ave[bin * kNumAvg + x] = a * (double)n;   // Histogram::SetAve
+        }
+      }
+    if (!is) { set_error("remd_histogram_read: truncated " + path); return REMD_ERR_IO; }
+    CK(cudaMemcpy(H.hist + nb * c, hist.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(H.ave + nb * kNumAvg * c, ave.data(), nb * kNumAvg * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(H.bounds + 5 * c, b, 5 * sizeof(int), cudaMemcpyHostToDevice));
   }
   return REMD_OK;
 }

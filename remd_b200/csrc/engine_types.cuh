@@ -107,6 +107,19 @@ struct DevPtrs {
   const int* changed;            // 1 = apply the exchange tail at the interval start
 };
 
-enum : int { kErrNbrOverflow = 1, kErrNonFinite = 2 };
+enum : int { kErrNbrOverflow = 1, kErrNonFinite = 2, kErrHistRange = 4 };
+
+// (volume, potential) histogram of the replicas of one ensemble, one per
+// condition slot (REMDInfo's Histogram, src/remdinfo.h:93-139): kHistBins x
+// kHistBins counts, per bin the sum of the 19 Average fields, and per slot the
+// occupied range {vmin, vmax, pmin, pmax, samples}.  hist == NULL: not kept.
+constexpr int kHistBins = 500;   // NUM_VOL = NUM_POT, src/remdinfo.h:22-23
+struct HistEns {
+  int* hist;       // [slot][v][p]
+  double* ave;     // [slot][v][p][kNumAvg]
+  int* bounds;     // [slot][5]
+  double emin, emax, de;   // kJ/mol per molecule
+  double vmin, vmax, dv;   // A^3 per molecule
+};
 
 }  // namespace remd

@@ -1581,6 +1581,58 @@ void launch_replica_rescale(const DevPtrs& d, RepState* X, bool per_step, cudaSt
   if (per_step) k_replica_rescale<true><<<d.nrep, kRepThreads, 0, s>>>(d, X);
   else k_replica_rescale<false><<<d.nrep, kRepThreads, 0, s>>>(d, X);
 }
+// ------------------------------------------------------------------ histograms
+// One thread per condition slot k (slot c of ensemble e).  The sample is the
+// Average of the replica at that condition, per molecule (src/remd.cxx:806-811):
+// p = (LJ + CLMB + WALL) / nmol, v = VOL / nmol.  Binning, range check and the
+// occupied-range bookkeeping follow REMDInfo::IncrementHistogram
+// (src/remdinfo.h:299-321) and Histogram::Increment (src/remdinfo.cxx:38-51);
+// KeepAverages adds the 19 fields to the bin.  A sample outside
+// [min, max) -- or one whose bin rounds up to kHistBins -- is not counted and
+// sets kErrHistRange (the reference exits there).  Each slot has one writer,
+// so no atomics are needed on the bins.
+__global__ void k_histogram(DevPtrs d, const HistEns* __restrict__ he, const int* __restrict__ rep_off,
+                            const int* __restrict__ index) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.nrep) return;
+  const int e = d.rc[k].ens;
+  const HistEns H = he[e];
+  if (!H.hist) return;
+  const int c = k - rep_off[e];
+  const int rep = rep_off[e] + index[k];
+  const double* a = d.avg + (long long)rep * kNumAvg;
+  const double nmol = (double)d.rc[rep].nmol;
+  const double pot = (a[0] + a[1] + a[2]) / nmol;
+  const double vol = a[3] / nmol;
+  bool ok = !(vol < H.vmin || vol >= H.vmax || pot < H.emin || pot >= H.emax);
+  const int v = ok ? (int)((vol - H.vmin) / H.dv) : 0;
+  const int p = ok ? (int)((pot - H.emin) / H.de) : 0;
+  ok = ok && v >= 0 && v < kHistBins && p >= 0 && p < kHistBins;
+  if (!ok) {
+    atomicOr(d.err, kErrHistRange);
+    return;
+  }
+  int* b = H.bounds + 5 * c;
+  if (b[4] == 0) {
+    b[0] = b[1] = v;
+    b[2] = b[3] = p;
+  }
+  b[0] = min(b[0], v);
+  b[1] = max(b[1], v);
+  b[2] = min(b[2], p);
+  b[3] = max(b[3], p);
+  b[4] += 1;
+  const long long bin = ((long long)c * kHistBins + v) * kHistBins + p;
+  H.hist[bin] += 1;
+  double* s = H.ave + bin * kNumAvg;
+  for (int x = 0; x < kNumAvg; x++) s[x] += a[x];
+}
+
+void launch_histogram(const DevPtrs& d, const HistEns* he, const int* rep_off, const int* index,
+                      cudaStream_t s) {
+  k_histogram<<<(d.nrep + 127) / 128, 128, 0, s>>>(d, he, rep_off, index);
+}
+
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, const unsigned long long* seeds,
                        int* index, double* T, double* P, long long* step_ctr, cudaStream_t s) {

@@ -38,6 +38,10 @@ void launch_replica_rescale(const DevPtrs& d, RepState* X, bool per_step, cudaSt
 void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, const int* u_off,
                        int nens, long step, const double* u, const unsigned long long* seeds,
                        int* index, double* T, double* P, long long* step_ctr, cudaStream_t s);
+// REMD::IncrementHistogram (src/remd.cxx:803-813) for every condition slot of the
+// ensembles with a histogram; index[slot] = the replica (ensemble-local) there.
+void launch_histogram(const DevPtrs& d, const HistEns* he, const int* rep_off, const int* index,
+                      cudaStream_t s);
 int pack_stride(int nsite, int prec);
 void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
                          cudaStream_t s);

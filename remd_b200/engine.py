@@ -26,7 +26,7 @@ NUM_AVG = 19
 AVG_NAMES = ["LJ", "CLMB", "WALL", "VOL", "TRA", "ROT", "T", "P", "Px", "Py", "Pz",
              "TOT", "DRF", "TSTs", "TSTv", "BSTx", "BSTy", "BSTz", "DUMMY"]
 STATUS = {0: "OK", 1: "INVALID", 2: "OOM", 3: "TIMEOUT", 4: "NONFINITE", 5: "CANCELLED",
-          6: "CUDA", 7: "IO", 8: "NEIGHBOR_OVERFLOW", 9: "NO_DEVICE"}
+          6: "CUDA", 7: "IO", 8: "NEIGHBOR_OVERFLOW", 9: "NO_DEVICE", 10: "RANGE"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -420,6 +420,34 @@ class REMDGPU:
         T, P = np.zeros(self.nrep), np.zeros(self.nrep)
         _check(lib().remd_get_conditions(self.h, _p(idx, _ip), _p(T), _p(P)))
         return idx, T, P
+
+    # ---- (volume, potential) histograms (REMDInfo's Histogram)
+    def histogram_enable(self, ens, energy_min, energy_max, volume_min, volume_max):
+        _check(lib().remd_histogram_enable(self.h, ens, C.c_double(energy_min), C.c_double(energy_max),
+                                           C.c_double(volume_min), C.c_double(volume_max)))
+
+    def histogram_increment(self, index=None):
+        """REMD::IncrementHistogram; index: slot -> replica, ensemble-local,
+        ensembles concatenated (None: the engine's own index)."""
+        if index is None:
+            _check(lib().remd_histogram_increment(self.h, None))
+        else:
+            idx = np.ascontiguousarray(index, dtype=np.int32)
+            _check(lib().remd_histogram_increment(self.h, _p(idx, _ip)))
+
+    def histogram(self, ens, slot):
+        """(bounds {vmin, vmax, pmin, pmax, samples}, counts (500, 500), per-bin sums (500, 500, 19))."""
+        b = np.zeros(5, dtype=np.int32)
+        hist = np.zeros((500, 500), dtype=np.int32)
+        ave = np.zeros((500, 500, 19))
+        _check(lib().remd_histogram_get(self.h, ens, slot, _p(b, _ip), _p(hist, _ip), _p(ave)))
+        return b, hist, ave
+
+    def histogram_write(self, ens, directory):
+        _check(lib().remd_histogram_write(self.h, ens, directory.encode()))
+
+    def histogram_read(self, ens, directory):
+        _check(lib().remd_histogram_read(self.h, ens, directory.encode()))
 
     def write_chk(self, rep, path):
         _check(lib().remd_write_chk(self.h, rep, path.encode()))

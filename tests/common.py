@@ -57,3 +57,23 @@ def golden_conditions():
 def rel(a, b):
     a, b = np.asarray(a, float), np.asarray(b, float)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# (volume, potential) histogram pins: energy_min, energy_max (kJ/mol per molecule),
+# volume_min, volume_max (A^3 per molecule), as in the .inp
+HIST_RANGES = (-60.0, -20.0, 25.0, 35.0)
+
+
+def histogram_samples(rng, nrep, nmol, nint):
+    """Seeded per-interval Average rows and slot -> replica permutations; the
+    potential and volume per molecule fall in [-41, -40) and [29.8, 30) so that
+    the written histograms stay small (about 12 x 10 bins)."""
+    out = []
+    for _ in range(nint):
+        avg = rng.normal(0.0, 1.0, (nrep, 19))
+        avg[:, 0] = rng.uniform(-5.0, -4.9, nrep) * nmol
+        avg[:, 1] = rng.uniform(-35.5, -35.0, nrep) * nmol
+        avg[:, 2] = rng.uniform(-0.4, -0.1, nrep) * nmol
+        avg[:, 3] = rng.uniform(29.8, 30.0, nrep) * nmol
+        out.append((rng.permutation(nrep).astype(np.int32), avg))
+    return out

@@ -4,10 +4,12 @@ Run in a container that has the reference sources (it builds oracle/_ref from
 them with oracle/Makefile):
 
     python tests/golden/make_golden.py [case ...]     (all cases when none is named)
+    python tests/golden/make_golden.py histograms     (ref_histograms.json only)
 
 Writes, next to this script:
   gpu0000.chk          copy of the reference's test input (test/input/gpu0000.chk)
   correct_line.json    the reference's golden interval-0 line (test/correct:4)
+  ref_histograms.json  the reference REMDInfo's histogram files for seeded samples
   ref_<case>.npz       for small seeded systems: the initial state and the
                        reference's own outputs (compiled reference CPU code,
                        generic FP64 build) after InitializeProperty (a force
@@ -60,8 +62,42 @@ def ref_outputs(ref, spec):
                                pr["tot"] - pr["wall"] + wall]))
 
 
+def histograms(path):
+    """ref_histograms.json: the reference REMDInfo's OutputHistogram files
+    (src/remdinfo.cxx:723-758) after REMD::IncrementHistogram-style feeding
+    (src/remd.cxx:803-813) of seeded samples (tests.common.histogram_samples)."""
+    import tempfile
+    from tests.common import HIST_RANGES, histogram_samples
+    seed, nt, npr, nmol, nint = 9, 3, 2, 50, 40
+    nrep = nt * npr
+    lib = O._ref_lib()
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = ("nmol %d\nntemp %d\nnpress %d\nnreplica %d\ntemp_min 250\ntemp_max 350\n"
+               "press_min 1e5\npress_max 2e8\npconstant 1\nconfined 0\ntconstant 1\n"
+               "energy_min %r\nenergy_max %r\nvolume_min %r\nvolume_max %r\n"
+               "output_prefix %s\ninput_prefix %s\n" % ((nmol, nt, npr, nrep) + HIST_RANGES + (tmp, tmp)))
+        h = lib.ref_remdinfo_create(inp.encode())
+        Tc, Pc = np.linspace(2.0, 3.0, nrep), np.linspace(0.01, 0.1, nrep)
+        for idx, avg in histogram_samples(np.random.default_rng(seed), nrep, nmol, nint):
+            T, P = np.zeros(nrep), np.zeros(nrep)
+            T[idx], P[idx] = Tc, Pc
+            lib.ref_remdinfo_set_arrays(h, O._ptr(idx, O._ip), O._ptr(T), O._ptr(P))
+            pot = np.ascontiguousarray(avg[:, 0] + avg[:, 1] + avg[:, 2])
+            vol = np.ascontiguousarray(avg[:, 3])
+            lib.ref_remdinfo_increment_histogram(h, O._ptr(pot), O._ptr(vol),
+                                                 O._ptr(np.ascontiguousarray(avg)))
+        lib.ref_remdinfo_output_histogram(h)
+        files = [open(O.Histograms.file_name(tmp, Pc[c], Tc[c])).read() for c in range(nrep)]
+    json.dump({"source": "REMDInfo::OutputHistogram (src/remdinfo.cxx:723-758)", "seed": seed,
+               "nrep": nrep, "nmol": nmol, "nint": nint, "ranges": list(HIST_RANGES),
+               "files": files}, open(path, "w"), indent=0)
+
+
 def main():
     O.build_oracle()
+    if sys.argv[1:] == ["histograms"]:
+        histograms(os.path.join(HERE, "ref_histograms.json"))
+        return
     shutil.copy(os.path.join(REF, "test/input/gpu0000.chk"), os.path.join(HERE, "gpu0000.chk"))
     with open(os.path.join(REF, "test/correct")) as f:
         line = f.read().splitlines()[3].split()

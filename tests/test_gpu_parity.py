@@ -503,3 +503,118 @@ def test_output_cdv_matches_restatement(tmp_path):
             k += 1
     assert not os.path.exists(f"{prefix}R{k:04d}s0000012.cdv")
     eng.close()
+
+
+def _hist_ranges(avg, nmol):
+    """energy / volume ranges per molecule that hold every sample of a short run."""
+    pot = (avg[:, 0] + avg[:, 1] + avg[:, 2]) / nmol
+    vol = avg[:, 3] / nmol
+    return (float(np.floor(pot.min()) - 40.0), float(np.ceil(pot.max()) + 40.0), 0.0,
+            float(np.ceil(vol.max()) * 1.5))
+
+
+def test_histograms_host_index_match_oracle_and_reference(tmp_path):
+    """remd_histogram_increment after each interval, with the conditions moved by
+    the host exchange: counts, bounds and per-bin sums equal the restatement
+    bit for bit, and remd_histogram_write gives the bytes the reference's
+    REMDInfo::OutputHistogram writes for the same samples."""
+    ens = [S.small_ensemble("tip4p", 1, nmol=96, ntemp=2, npress=2, seed=71, interval=10),
+           S.small_ensemble("tip3p", 0, nmol=64, ntemp=3, npress=1, seed=72, interval=10)]
+    eng = E.REMDGPU(ens, precision="fp32")
+    offs = np.cumsum([0] + [e.nreplica for e in ens])
+    a0 = eng.all_averages()
+    ranges = [_hist_ranges(a0[offs[i]:offs[i + 1]], e.spec.nmol) for i, e in enumerate(ens)]
+    eng.histogram_enable(0, *ranges[0])          # ensemble 1 keeps none
+    orc = O.Histograms(ens[0].nreplica, *ranges[0])
+    idx = [np.arange(e.nreplica, dtype=np.int32) for e in ens]
+    T = [e.T.copy() for e in ens]
+    P = [e.P.copy() for e in ens]
+    rng = np.random.default_rng(3)
+    samples = []
+    for step in range(6):
+        eng.ExecuteSteps(np.concatenate(T), np.concatenate(P))
+        avg = eng.all_averages()
+        eng.histogram_increment(np.concatenate(idx))
+        a = avg[offs[0]:offs[1]]
+        orc.increment(idx[0], a, ens[0].spec.nmol)
+        samples.append((idx[0].copy(), T[0].copy(), P[0].copy(), a.copy()))
+        for i, e in enumerate(ens):
+            ai = avg[offs[i]:offs[i + 1]]
+            O.replica_exchange(e.ntemp, e.npress, e.spec.pconstant, step, idx[i], T[i], P[i],
+                               ai[:, 0] + ai[:, 1] + ai[:, 2], ai[:, 3], rng.random(e.nreplica))
+    for c in range(ens[0].nreplica):
+        b, hist, ave = eng.histogram(0, c)
+        assert np.array_equal(b, orc.bounds[c]) and np.array_equal(hist, orc.hist[c])
+        assert np.array_equal(ave, orc.ave[c])
+    out = tmp_path / "eng"
+    out.mkdir()
+    eng.histogram_write(0, str(out))
+    # the slot's condition is that of the replica the slot's index names
+    Tc, Pc = T[0][idx[0]], P[0][idx[0]]
+    for c in range(ens[0].nreplica):
+        assert open(O.Histograms.file_name(str(out), Pc[c], Tc[c])).read() == orc.text(c)
+    if O.reference_available():
+        lib = O._ref_lib()
+        ref = tmp_path / "ref"
+        ref.mkdir()
+        e = ens[0]
+        inp = ("nmol %d\nntemp %d\nnpress %d\nnreplica %d\ntemp_min 250\ntemp_max 350\n"
+               "press_min 1e5\npress_max 2e8\npconstant %d\nconfined 1\ntconstant 1\n"
+               "energy_min %r\nenergy_max %r\nvolume_min %r\nvolume_max %r\n"
+               "output_prefix %s\ninput_prefix %s\n"
+               % ((e.spec.nmol, e.ntemp, e.npress, e.nreplica, e.spec.pconstant) + tuple(ranges[0]) + (ref, ref)))
+        h = lib.ref_remdinfo_create(inp.encode())
+        for ix, Ts, Ps, a in samples:
+            lib.ref_remdinfo_set_arrays(h, O._ptr(ix, O._ip), O._ptr(Ts), O._ptr(Ps))
+            pot = np.ascontiguousarray(a[:, 0] + a[:, 1] + a[:, 2])
+            vol = np.ascontiguousarray(a[:, 3])
+            lib.ref_remdinfo_increment_histogram(h, O._ptr(pot), O._ptr(vol), O._ptr(np.ascontiguousarray(a)))
+        lib.ref_remdinfo_set_arrays(h, O._ptr(idx[0], O._ip), O._ptr(T[0]), O._ptr(P[0]))
+        lib.ref_remdinfo_output_histogram(h)
+        for c in range(e.nreplica):
+            name = os.path.basename(O.Histograms.file_name("", Pc[c], Tc[c]))
+            assert open(ref / name).read() == open(out / name).read()
+    # ReadHistogramFromBackUp: counts and bounds back exactly, sums to the file's 7 digits
+    eng.histogram_enable(0, *ranges[0])
+    eng.histogram_read(0, str(out))
+    for c in range(ens[0].nreplica):
+        b, hist, ave = eng.histogram(0, c)
+        assert np.array_equal(b, orc.bounds[c]) and np.array_equal(hist, orc.hist[c])
+        assert np.allclose(ave, orc.ave[c], rtol=1e-6, atol=1e-300)
+    with pytest.raises(E.RemdError, match="INVALID"):
+        eng.histogram(1, 0)
+    eng.close()
+
+
+def test_histograms_in_the_interval_graph():
+    """With the device exchange on, the interval graph samples every slot before
+    exchanging (one more launch per interval); the result equals the restatement
+    fed with the slot -> replica index each interval started from."""
+    e = S.small_ensemble("tip5p", 2, nmol=80, ntemp=2, npress=2, seed=73, interval=10)
+    eng = E.REMDGPU([e], precision="fp32")
+    ranges = _hist_ranges(eng.all_averages(), e.spec.nmol)
+    n0 = eng.launches_per_interval()
+    eng.enable_device_exchange([(e.ntemp, e.npress)], seed=11)
+    eng.histogram_enable(0, *ranges)
+    assert eng.launches_per_interval() == n0 + 2
+    orc = O.Histograms(e.nreplica, *ranges)
+    for _ in range(8):
+        idx_pre = eng.conditions()[0]
+        eng.execute_device()
+        orc.increment(idx_pre, eng.all_averages(), e.spec.nmol)
+    for c in range(e.nreplica):
+        b, hist, ave = eng.histogram(0, c)
+        assert np.array_equal(b, orc.bounds[c]) and np.array_equal(hist, orc.hist[c])
+        assert np.array_equal(ave, orc.ave[c])
+    assert orc.bounds[:, 4].sum() == 8 * e.nreplica
+    eng.close()
+
+
+def test_histogram_sample_out_of_range_is_an_error():
+    e = S.small_ensemble("tip4p", 0, nmol=64, ntemp=2, npress=1, seed=74, interval=5)
+    eng = E.REMDGPU([e], precision="fp32")
+    eng.histogram_enable(0, 100.0, 200.0, 0.0, 1.0)   # no water sits there
+    eng.ExecuteSteps(e.T, e.P)
+    with pytest.raises(E.RemdError, match="RANGE"):
+        eng.histogram_increment(np.arange(e.nreplica))
+    eng.close()

@@ -2,11 +2,13 @@
 it against (a) fixtures the reference itself produced (tests/golden/ref_*.npz,
 made by tests/golden/make_golden.py) and (b) the compiled reference, when
 oracle/_ref is present."""
+import os
+
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.common import CASES, NSTEPS, load_case, rel
+from tests.common import CASES, GOLDEN, HIST_RANGES, NSTEPS, histogram_samples, load_case, rel
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -137,3 +139,48 @@ def test_cdv_restatement_known_answer():
     assert bulk.startswith("' box_sx=-10 box_sy=-10 box_sz=-15 box_ex=10 box_ey=10 box_ez=15 ")
     slit = O.cdv_text(r[:1], q[:1], [20.0, 20.0, 30.0], [[0.0, 0.0, 0.0]], 2.5, 0.0625, 2, 9.0)
     assert slit.startswith("' box_sx=-10 box_sy=-10 box_sz=-4.5 box_ex=10 box_ey=10 box_ez=4.5 ")
+
+
+def test_histogram_restatement_matches_golden():
+    """The restatement against the reference REMDInfo's own histogram files for
+    the seeded samples (tests/golden/ref_histograms.json, make_golden.py)."""
+    import json
+    g = json.load(open(os.path.join(GOLDEN, "ref_histograms.json")))
+    orc = O.Histograms(g["nrep"], *g["ranges"])
+    for idx, avg in histogram_samples(np.random.default_rng(g["seed"]), g["nrep"], g["nmol"], g["nint"]):
+        orc.increment(idx, avg, g["nmol"])
+    for c in range(g["nrep"]):
+        assert orc.text(c) == g["files"][c], c
+
+
+def test_histogram_restatement_matches_reference_remdinfo(tmp_path):
+    """REMD::IncrementHistogram + REMDInfo::OutputHistogram: the restatement and
+    the reference's compiled REMDInfo, fed the same samples, write the same bytes."""
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    nt, npr, nmol = 3, 2, 50
+    nrep = nt * npr
+    inp = ("nmol %d\nntemp %d\nnpress %d\nnreplica %d\ntemp_min 250\ntemp_max 350\n"
+           "press_min 1e5\npress_max 2e8\npconstant 1\nconfined 0\ntconstant 1\n"
+           "energy_min -60\nenergy_max -20\nvolume_min 25\nvolume_max 35\n"
+           "output_prefix %s\ninput_prefix %s\n" % (nmol, nt, npr, nrep, tmp_path, tmp_path))
+    lib = O._ref_lib()
+    h = lib.ref_remdinfo_create(inp.encode())
+    Tc = np.linspace(2.0, 3.0, nrep)
+    Pc = np.linspace(0.01, 0.1, nrep)
+    orc = O.Histograms(nrep, *HIST_RANGES)
+    rng = np.random.default_rng(9)
+    for idx, avg in histogram_samples(rng, nrep, nmol, 40):
+        T = np.zeros(nrep)
+        P = np.zeros(nrep)
+        T[idx], P[idx] = Tc, Pc           # replica idx[c] holds condition c
+        lib.ref_remdinfo_set_arrays(h, O._ptr(idx, O._ip), O._ptr(T), O._ptr(P))
+        pot = np.ascontiguousarray(avg[:, 0] + avg[:, 1] + avg[:, 2])
+        vol = np.ascontiguousarray(avg[:, 3])
+        lib.ref_remdinfo_increment_histogram(h, O._ptr(pot), O._ptr(vol), O._ptr(np.ascontiguousarray(avg)))
+        orc.increment(idx, avg, nmol)
+    lib.ref_remdinfo_output_histogram(h)
+    for c in range(nrep):
+        ref = open(O.Histograms.file_name(str(tmp_path), Pc[c], Tc[c])).read()
+        assert ref == orc.text(c), c
+    assert orc.bounds[:, 4].sum() == 40 * nrep
