@@ -62,19 +62,30 @@ __device__ inline double warp_max(double v) {
 }
 
 // Sum of the force partials of replica c (ordered pairs -> halved like
-// ForceCalculator::Switching, src/force_calculator.cxx:775-778).
-__device__ inline void reduce_part2(const DevPtrs& d, const RepConst& c, double& lj, double& clmb,
-                                    double& wall, double* vir) {
-  double a = 0, b = 0, w = 0, v0 = 0, v1 = 0, v2 = 0;
-  for (int t = c.warp_off; t < c.warp_off + c.nwarp; t++) {
+// ForceCalculator::Switching, src/force_calculator.cxx:775-778).  Called by
+// all 32 lanes of one warp: lane l sums records l, l+32, ..., then a butterfly
+// over the lanes.  Every lane ends with the same bits (the two partners of a
+// butterfly step add the same two numbers) and the order depends only on the
+// replica's record count, so every kernel that needs the sums gets identical
+// values.  One warp loads all records at once instead of one thread walking
+// them: the per-replica scalar chains of the step kernels start sooner.
+struct P2Sum {
+  double lj, clmb, wall, vir[3];
+};
+__device__ inline P2Sum reduce_part2(const DevPtrs& d, const RepConst& c) {
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (int t = c.warp_off + (threadIdx.x & 31); t < c.warp_off + c.nwarp; t += 32) {
     const Part2 p = d.part2[t];
-    a += p.lj; b += p.clmb; w += p.wall;
-    v0 += p.vir[0]; v1 += p.vir[1]; v2 += p.vir[2];
+    v[0] += p.lj; v[1] += p.clmb; v[2] += p.wall;
+    v[3] += p.vir[0]; v[4] += p.vir[1]; v[5] += p.vir[2];
   }
-  lj = a * 0.5;
-  clmb = b * 0.5;
-  wall = w;
-  vir[0] = v0 * 0.5; vir[1] = v1 * 0.5; vir[2] = v2 * 0.5;
+  warp_sum<6>(v);
+  P2Sum e;
+  e.lj = v[0] * 0.5;
+  e.clmb = v[1] * 0.5;
+  e.wall = v[2];
+  e.vir[0] = v[3] * 0.5; e.vir[1] = v[4] * 0.5; e.vir[2] = v[5] * 0.5;
+  return e;
 }
 
 // Difference of two fixed-point box fractions with 32-bit wraparound: the
@@ -144,26 +155,26 @@ struct StepCoef {
 };
 
 template <bool MID>
-__global__ void __launch_bounds__(256) k_integrate(DevPtrs d, const RepState* __restrict__ X,
+__global__ void __launch_bounds__(128, 7) k_integrate(DevPtrs d, const RepState* __restrict__ X,
                                                    RepState* __restrict__ Y, int prec) {
   __shared__ StepCoef sc;
   const Tile t = d.tiles[blockIdx.x];
   const RepConst& c = d.rc[t.rep];
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
     RepState st = X[t.rep];
-    double lj, clmb, wall, vir[3];
-    reduce_part2(d, c, lj, clmb, wall, vir);
-    const double pot = lj + clmb + wall;
+    const double pot = e.lj + e.clmb + e.wall;
     if (MID) {   // D5 (scalar) + D6 closing the previous step
       for (int x = 0; x < 3; x++) sc.coef_v_a[x] = st.L[x] * st.s * c.dthalf;
       sc.coef_p_a = 2.0 * st.s * c.dthalf;
-      d5_scalar(c, st, pot, vir);
+      d5_scalar(c, st, pot, e.vir);
       d6(c, st);
     }
     d6(c, st);   // D6 opening this step
     for (int x = 0; x < 3; x++) sc.coef_v_c[x] = st.L[x] * st.s * c.dthalf;
     sc.coef_p_c = 2.0 * st.s * c.dthalf;
-    d5_scalar(c, st, pot, vir);
+    d5_scalar(c, st, pot, e.vir);
     d4(c, st);
     sc.coef_xi = 0.25 / st.s;
     const double si = 1.0 / st.s;
@@ -628,19 +639,21 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const F32Cons
             ecl += e;
             ftmp += e * ri2;
           }
-          ftmp *= sw;
           tx += x * ftmp; ty += y * ftmp; tz += z * ftmp;
         }
-        fs[kk][0] += tx; fs[kk][1] += ty; fs[kk][2] += tz;
+        // the switch multiplies the site forces once per site (FFMA into the sums)
+        fs[kk][0] = fmaf(sw, tx, fs[kk][0]);
+        fs[kk][1] = fmaf(sw, ty, fs[kk][1]);
+        fs[kk][2] = fmaf(sw, tz, fs[kk][2]);
         fpx += tx; fpy += ty; fpz += tz;
       }
       const float e = elj + ecl;
       const float g = dsw * rinv * e;
       const float cx = -dx * g, cy = -dy * g, cz = -dz * g;
       fc[0] += cx; fc[1] += cy; fc[2] += cz;
-      fv[0] += (fpx + cx) * dx;
-      fv[1] += (fpy + cy) * dy;
-      fv[2] += (fpz + cz) * dz;
+      fv[0] += fmaf(fpx, sw, cx) * dx;
+      fv[1] += fmaf(fpy, sw, cy) * dy;
+      fv[2] += fmaf(fpz, sw, cz) * dz;
       flj += sw * elj;
       fcl += sw * ecl;
       if ((++done & 15) == 0) { flush(); zero(); }
@@ -935,21 +948,30 @@ __device__ void force_tile_f32(const DevPtrs& d, const RepConst& c, const Tile& 
   write_part2(d, c, t, a, wall_e);
 }
 
-// Head of a force step (thread 0): PsPv and D4 with the integrate kernel's
-// partials (src/integrator.cxx:132-172, 604-632), the replica's new scalars to
-// Xout (first tile), and whether this tile's skin list must be rebuilt.
+// Head of a force step (warp 0; lane 0 finishes): PsPv and D4 with the
+// integrate kernel's partials (src/integrator.cxx:132-172, 604-632), the
+// replica's new scalars to Xout (first tile), and whether this tile's skin
+// list must be rebuilt.  The partials are summed like reduce_part2 (lane-strided,
+// then a butterfly), so every tile of a replica gets the same bits.
 template <bool FORCE_ONLY>
 __device__ void force_head(const DevPtrs& d, const RepConst& c, int rep, int tix, const RepState* Yin,
                            RepState* Xout, ForceHead& h) {
-  RepState st = Yin[rep];
+  double v[4] = {0, 0, 0, 0}, disp = 0.0;
   if (!FORCE_ONLY) {
-    double sPv[3] = {0, 0, 0}, sPs = 0.0, disp = 0.0;
-    for (int k = c.warp_off; k < c.warp_off + c.nwarp; k++) {
+    for (int k = c.warp_off + (threadIdx.x & 31); k < c.warp_off + c.nwarp; k += 32) {
       const Part1 p = d.part1[k];
-      sPv[0] += p.sum_Pv[0]; sPv[1] += p.sum_Pv[1]; sPv[2] += p.sum_Pv[2];
-      sPs += p.sum_Ps;
+      v[0] += p.sum_Pv[0]; v[1] += p.sum_Pv[1]; v[2] += p.sum_Pv[2];
+      v[3] += p.sum_Ps;
       disp = fmax(disp, p.disp);
     }
+    warp_sum<4>(v);
+    disp = warp_max(disp);
+  }
+  if ((threadIdx.x & 31) != 0) return;
+  RepState st = Yin[rep];
+  if (!FORCE_ONLY) {
+    double sPv[3] = {v[0], v[1], v[2]};
+    const double sPs = v[3];
     pspv(c, st, sPv, sPs);
     d4(c, st);
     if (tix == c.tile_off) Xout[rep] = st;
@@ -976,7 +998,7 @@ __global__ void __launch_bounds__(128) k_force_f64(DevPtrs d, const RepState* __
   const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;   // costliest tiles first
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
-  if (threadIdx.x == 0) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
+  if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
   __syncthreads();
   const double L[3] = {h.L[0], h.L[1], h.L[2]};
   const bool rb = h.rebuild != 0;
@@ -997,7 +1019,7 @@ __global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepStat
   const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
-  if (threadIdx.x == 0) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
+  if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
   __syncthreads();
   const double L[3] = {h.L[0], h.L[1], h.L[2]};
   const int i = threadIdx.x;
@@ -1049,9 +1071,9 @@ __device__ inline double barostat_energy(const RepConst& c, const RepState& st) 
 // Molecules::CalcProperties (src/molecules.cxx:702-734) from the reduced kinetic
 // sums; writes the REMDGPU::GetAverages fields (T and pressures reduced).
 __device__ inline double calc_properties(const DevPtrs& d, const RepConst& c, const RepState& st,
-                                         const double* tra3raw, double rot, double* avg) {
-  double lj, clmb, wall, vir[3];
-  reduce_part2(d, c, lj, clmb, wall, vir);
+                                         const double* tra3raw, double rot, double* avg, const P2Sum& e) {
+  const double lj = e.lj, clmb = e.clmb, wall = e.wall;
+  const double* vir = e.vir;
   const double pot = lj + clmb + wall;
   double tmp[3];
   for (int x = 0; x < 3; x++) {
@@ -1111,13 +1133,13 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_end(DevPtrs d, RepState
   __shared__ double red[8 * 4];
   const int rep = blockIdx.x;
   const RepConst& c = d.rc[rep];
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
     RepState s = X[rep];
-    double lj, clmb, wall, vir[3];
-    reduce_part2(d, c, lj, clmb, wall, vir);
     for (int x = 0; x < 3; x++) cv[x] = s.L[x] * s.s * c.dthalf;
     cv[3] = 2.0 * s.s * c.dthalf;
-    d5_scalar(c, s, lj + clmb + wall, vir);
+    d5_scalar(c, s, e.lj + e.clmb + e.wall, e.vir);
     d6(c, s);
     st = s;
   }
@@ -1137,7 +1159,7 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_end(DevPtrs d, RepState
   kinetic_sums(d, c, st.s, acc);
   block_sum<4>(acc, red);
   if (threadIdx.x == 0) {
-    calc_properties(d, c, st, acc, acc[3], d.avg + (long long)rep * kNumAvg);
+    calc_properties(d, c, st, acc, acc[3], d.avg + (long long)rep * kNumAvg, e);
     X[rep] = st;
     finish_replica(d, c, rep, st);
   }
@@ -1153,10 +1175,12 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_props(DevPtrs d, RepSta
   double acc[4];
   kinetic_sums(d, c, st.s, acc);
   block_sum<4>(acc, red);
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
     st.gkT = 6.0 * (double)c.nmol * st.T;
     double* avg = d.avg + (long long)rep * kNumAvg;
-    st.H0 = calc_properties(d, c, st, acc, acc[3], avg);
+    st.H0 = calc_properties(d, c, st, acc, acc[3], avg, e);
     avg[12] = 0.0;
     X[rep] = st;
   }
@@ -1263,10 +1287,12 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_start(DevPtrs d, RepSta
   double kacc[4];
   kinetic_sums(d, c, st.s, kacc);
   block_sum<4>(kacc, red);
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
     RepState s = st;
     s.P = Pn;
-    s.H0 = calc_properties(d, c, s, kacc, kacc[3], nullptr);
+    s.H0 = calc_properties(d, c, s, kacc, kacc[3], nullptr, e);
     X[rep] = s;
   }
 }
@@ -1343,11 +1369,13 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_rescale(DevPtrs d, RepS
   }
   kinetic_sums(d, c, st.s, k);
   block_sum<4>(k, red);
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
     RepState s = st;
     s.gkT = 6.0 * (double)c.nmol * s.T;
     double* avg = d.avg + (long long)rep * kNumAvg;
-    s.H0 = calc_properties(d, c, s, k, k[3], avg);
+    s.H0 = calc_properties(d, c, s, k, k[3], avg, e);
     avg[12] = 0.0;
     X[rep] = s;
   }
@@ -1514,13 +1542,13 @@ __global__ void k_noalloc_store(DevPtrs d, double* __restrict__ f_aos, double* _
     for (int x = 0; x < 3; x++) f_aos[3 * li + x] = d.f[x * d.N + g];
     for (int x = 0; x < 4; x++) n_aos[4 * li + x] = d.n[x * d.N + g];
   }
+  P2Sum e;
+  if (threadIdx.x < 32) e = reduce_part2(d, c);
   if (threadIdx.x == 0) {
-    double lj, clmb, wall, vir[3];
-    reduce_part2(d, c, lj, clmb, wall, vir);
     long long np = 0;
     for (int t = c.warp_off; t < c.warp_off + c.nwarp; t++) np += d.part2[t].npairs;
-    out[0] = lj; out[1] = clmb; out[2] = wall;
-    out[3] = vir[0]; out[4] = vir[1]; out[5] = vir[2];
+    out[0] = e.lj; out[1] = e.clmb; out[2] = e.wall;
+    out[3] = e.vir[0]; out[4] = e.vir[1]; out[5] = e.vir[2];
     out[6] = (double)(np / 2);
     out[7] = (double)*d.err;
   }
