@@ -624,9 +624,8 @@ def engine_arm(args, rank, world, local):
         Ps = [e.P.copy() for e in ens]
         rng = np.random.default_rng(123 + rank)
         off = np.cumsum([0] + [e.nreplica for e in ens])
-        barrier(world)
-        t0 = time.perf_counter()
-        for step in range(args.steps):
+
+        def interval(step):
             eng.ExecuteSteps(np.concatenate(Ts), np.concatenate(Ps))
             avg = eng.all_averages()
             for i, e in enumerate(ens):
@@ -634,6 +633,13 @@ def engine_arm(args, rank, world, local):
                 E.exchange_host(grids[i][0], grids[i][1], e.spec.pconstant, step, idx[i], Ts[i],
                                 Ps[i], a[:, 0] + a[:, 1] + a[:, 2], a[:, 3],
                                 rng.random(max(e.nreplica // 2, 1)))
+        # untimed: the first call re-instantiates the interval graph (without the
+        # device exchange that the device-timed loop used)
+        interval(0)
+        barrier(world)
+        t0 = time.perf_counter()
+        for step in range(args.steps):
+            interval(step + 1)
         e2e_s = reduce_max(time.perf_counter() - t0, world)
         e2e = {"value": total_units / e2e_s, "unit": METRIC,
                "h2d_bytes_per_step": int(2 * 8 * eng.nrep),

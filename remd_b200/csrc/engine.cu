@@ -1204,15 +1204,11 @@ static remd_status slot_conditions(remd_engine_s* h, int e, std::vector<double>&
   std::vector<int> idx(h->nrep);
   std::vector<double> T(h->nrep), P(h->nrep);
   CK(cudaStreamSynchronize(h->stream));
-  if (h->exch_enabled) {
-    CK(cudaMemcpy(idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(T.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(P.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
-  } else {
-    idx = h->h_hidx;
-    T = h->curT;
-    P = h->curP;
-  }
+  // the conditions of the last interval (the device exchange updates them in place)
+  CK(cudaMemcpy(T.data(), h->dT, h->nrep * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(P.data(), h->dP, h->nrep * 8, cudaMemcpyDeviceToHost));
+  if (h->exch_enabled) CK(cudaMemcpy(idx.data(), h->d_index, h->nrep * 4, cudaMemcpyDeviceToHost));
+  else idx = h->h_hidx;
   const int off = h->ens_rep_off[e], n = h->ens_nrep[e];
   Tc.resize(n);
   Pc.resize(n);
