@@ -553,7 +553,9 @@ def engine_arm(args, rank, world, local):
     if args.tile or args.skin:
         tuning = {"tile": args.tile or 64, "skin": args.skin or 1.0, "autotuned": False}
     else:
-        t, k, tms = eng.autotune(nsteps=20)
+        # 100 steps per trial: each trial starts with a list build, which a shorter
+        # window over-weights (it favours the largest skin)
+        t, k, tms = eng.autotune(nsteps=100)
         tuning = {"tile": t, "skin": k, "autotuned": True, "ms_per_md_step": tms}
     # one bench step = one REMD interval: `interval` MD steps of every replica and
     # the Metropolis exchange of every ensemble, all on the device
@@ -597,7 +599,7 @@ def engine_arm(args, rank, world, local):
             flops += pr * FLOP_PER_PAIR[e.spec.moltype.nsite]
             k += 1
     prof = (ctypes.c_double * 2)()
-    E._check(E.lib().remd_profile_steps(eng.h, 10, prof))
+    E._check(E.lib().remd_profile_steps(eng.h, 50, prof))   # 50 steps: list rebuilds at their usual rate
     force_ms, integ_ms = prof[1], prof[0]
     peak = ctypes.c_double()
     E._check(E.lib().remd_measure_fp32_peak(dev, ctypes.byref(peak)))
