@@ -704,7 +704,7 @@ remd_status remd_autotune(remd_handle h, int nsteps, int* tile_out, double* skin
   remd_status s = save_state(h, sv);
   if (s != REMD_OK) return s;
   static const int tiles[] = {32, 64, 96, 128};
-  static const double skins[] = {0.4, 0.6, 0.8, 1.0, 1.4};
+  static const double skins[] = {0.2, 0.4, 0.6, 0.8, 1.0, 1.4};
   int best_tile = h->tile;
   double best_skin = h->skin, best_ms = 1e300;
   for (int t : tiles)

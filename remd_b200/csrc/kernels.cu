@@ -253,6 +253,13 @@ struct ForceHead {
 // Neighbour-list rebuild for the molecules of this tile: every molecule of the
 // replica is tested against (rcut+skin), 128 candidates at a time from shared
 // memory (all lanes read the same candidate: a broadcast).
+// FP32 form: the skin list only has to contain every pair within rcut+skin
+// (pass 1 then keeps exactly the pairs within rcut), so the test is a
+// conservative one in FP32 on the top 16 bits of each fixed-point difference
+// (converted with the 1.5*2^23 bit trick, on the FMA pipe), against
+// rcut+skin widened by the truncation error sqrt(3) L_max 2^-16 and a relative
+// 1e-5.  It may keep a few pairs just beyond rcut+skin; the lists, and
+// therefore the results, of pass 1 do not change.
 template <int PREC>
 __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                             uint16_t* nb, int tile_size) {
@@ -265,6 +272,14 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
   int cnt = 0;
   int ix = 0, iy = 0, iz = 0;
   double rx = 0, ry = 0, rz = 0;
+  const float lsc0 = (float)(L[0] * (1.0 / 65536.0)), lsc1 = (float)(L[1] * (1.0 / 65536.0)),
+              lsc2 = (float)(L[2] * (1.0 / 65536.0));
+  float rl2f = 0.f;
+  if (PREC == kF32) {
+    const double lmax = fmax(fmax(L[0], L[1]), L[2]);
+    const double rw = (rl + 1.7320508075688772 * lmax * (1.0 / 65536.0)) * (1.0 + 1e-5);
+    rl2f = (float)(rw * rw);
+  }
   if (valid) {
     if (PREC == kF32) {
       const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
@@ -290,13 +305,19 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
       const int nk = min(128, c.nmol - base);
       for (int k = 0; k < nk; k++) {
         const int j = base + k;
-        double dx, dy, dz;
         if (PREC == kF32) {
           const int4 cj = reinterpret_cast<const int4*>(&cand[k])[0];
-          dx = (double)wrap_diff(ix, cj.x) * kFixInv * L[0];
-          dy = (double)wrap_diff(iy, cj.y) * kFixInv * L[1];
-          dz = (double)wrap_diff(iz, cj.z) * kFixInv * L[2];
-        } else {
+          const float fx = (__int_as_float(0x4B400000 + (wrap_diff(ix, cj.x) >> 16)) - 12582912.f) * lsc0;
+          const float fy = (__int_as_float(0x4B400000 + (wrap_diff(iy, cj.y) >> 16)) - 12582912.f) * lsc1;
+          const float fz = (__int_as_float(0x4B400000 + (wrap_diff(iz, cj.z) >> 16)) - 12582912.f) * lsc2;
+          if (j != li && fx * fx + fy * fy + fz * fz < rl2f) {
+            if (cnt < c.nbr_cap) nb[(long long)cnt * tile_size] = (uint16_t)j;
+            cnt++;
+          }
+          continue;
+        }
+        double dx, dy, dz;
+        {
           const double4 cj = cand[k];
           dx = (rx - cj.x) * L[0];
           dy = (ry - cj.y) * L[1];
