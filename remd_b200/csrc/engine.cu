@@ -33,6 +33,8 @@ using namespace remd;
 struct remd_engine_s {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;      // second chain of the interval graph
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int prec = kF32;
   int tile = 128;
   double skin = 1.0;
@@ -42,6 +44,9 @@ struct remd_engine_s {
   std::vector<RepConst> rc;
   std::vector<Tile> tiles;
   std::vector<int> order;          // force blocks -> tiles, costliest first
+  std::vector<int> order2;         // the same per half: tiles [0, split_tile), then the rest
+  int split_tile = 0;              // 0: the interval graph runs one chain
+  int* d_order2 = nullptr;
   std::vector<double> curT, curP;
   std::vector<double> wall_h;
   DevPtrs d{};
@@ -162,6 +167,26 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
     h->order.resize(h->tiles.size());
     for (size_t t = 0; t < h->order.size(); t++) h->order[t] = (int)t;
     std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    // two halves of the replicas (split at the replica boundary nearest half the
+    // cost) for the two independent chains of the interval graph
+    h->split_tile = 0;
+    if (h->nrep >= 2) {
+      double tot = 0.0, run = 0.0;
+      for (double x : cost) tot += x;
+      int best = 0;
+      double bestd = 1e300;
+      for (int r = 1; r < h->nrep; r++) {
+        const RepConst& pc = h->rc[r - 1];
+        for (int t = pc.tile_off; t < pc.tile_off + pc.ntile; t++) run += cost[t];
+        const double dd = std::fabs(run - 0.5 * tot);
+        if (dd < bestd) { bestd = dd; best = h->rc[r].tile_off; }
+      }
+      h->split_tile = best;
+    }
+    h->order2.clear();
+    for (int half = 0; half < 2; half++)
+      for (int t : h->order)
+        if ((t < h->split_tile) == (half == 0)) h->order2.push_back(t);
   }
   const size_t N = h->N, nt = h->tiles.size(), nr = h->nrep;
   const size_t elem = (h->prec == kF32) ? 4 : 8;
@@ -189,6 +214,7 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       nt * 4,                          // 31 order
       (h->prec == kF32) ? N * 4 : 0,   // 32 nt_cnt (FP32 per-step list counts)
       N * sizeof(int4),                // 33 com (FP32 current fixed-point centres)
+      nt * 4,                          // 34 order per half (two-chain interval graph)
   };
   offs.clear();
   total = 0;
@@ -252,11 +278,14 @@ static remd_status allocate(remd_engine_s* h) {
   d.order = reinterpret_cast<int*>(b + offs[31]);
   d.nt_cnt = reinterpret_cast<int*>(b + offs[32]);
   d.com = reinterpret_cast<int4*>(b + offs[33]);
+  d.tile0 = 0;
+  h->d_order2 = reinterpret_cast<int*>(b + offs[34]);
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync((void*)d.tiles, h->tiles.data(), h->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync((void*)d.order, h->order.data(), h->order.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_order2, h->order2.data(), h->order2.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   if (!h->wall_h.empty())
     CK(cudaMemcpyAsync((void*)d.wall, h->wall_h.data(), h->wall_h.size() * 8, cudaMemcpyHostToDevice, h->stream));
   // later set-up copies use the default stream, which does not order with this
@@ -326,9 +355,32 @@ static remd_status build_graph(remd_engine_s* h) {
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   launch_replica_start(h->d, h->X, h->stream);
-  for (int s = 0; s < h->interval; s++) {
-    launch_step_integrate(h, s);
-    launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
+  if (h->split_tile > 0 && !h->vscale) {
+    // two independent chains, one per half of the replicas (no data crosses
+    // between them), so one half's latency-bound phases -- the integrate
+    // kernel's scalar chains, the list kernel's heads, the pair kernel's tail
+    // -- overlap the other half's work
+    DevPtrs dA = h->d, dB = h->d;
+    dA.ntiles = h->split_tile;
+    dA.order = h->d_order2;
+    dB.ntiles = h->d.ntiles - h->split_tile;
+    dB.order = h->d_order2 + h->split_tile;
+    dB.tile0 = h->split_tile;
+    cudaEventRecord(h->ev_fork, h->stream);
+    cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
+    for (int s = 0; s < h->interval; s++) {
+      launch_integrate_prec(dA, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
+      launch_force(dA, h->Y, h->X, h->prec, false, h->tile, h->stream);
+      launch_integrate_prec(dB, h->X, h->Y, s > 0, h->tile, h->prec, h->stream2);
+      launch_force(dB, h->Y, h->X, h->prec, false, h->tile, h->stream2);
+    }
+    cudaEventRecord(h->ev_join, h->stream2);
+    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+  } else {
+    for (int s = 0; s < h->interval; s++) {
+      launch_step_integrate(h, s);
+      launch_force(h->d, h->Y, h->X, h->prec, false, h->tile, h->stream);
+    }
   }
   launch_replica_end(h->d, h->X, h->stream);
   // the histogram samples the interval before the exchange moves the conditions
@@ -553,6 +605,9 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   h->nrep = rep;
   h->N = mol;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
       force_kernel_setup() != cudaSuccess) {
     set_error("cannot set up device/stream");
     delete h;
@@ -616,6 +671,9 @@ remd_status remd_destroy(remd_handle h) {
   }
   if (h->d_hist) cudaFree(h->d_hist);
   if (h->d_hidx) cudaFree(h->d_hidx);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return REMD_OK;
@@ -857,7 +915,9 @@ int remd_launches_per_interval(remd_handle h) {
   // with velocity scaling also the rescale and, after the first step, the closing kick)
   // + replica_end + the device exchange when enabled (and the histogram before it)
   if (!h) return 0;
-  const int per_step = (h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0);
+  // (the two-chain graph, without velocity scaling, launches each step kernel once per half)
+  const bool split = h->split_tile > 0 && !h->vscale;
+  const int per_step = ((h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0)) * (split ? 2 : 1);
   return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0) +
          (h->exch_enabled && h->hist_on ? 1 : 0);
 }

@@ -105,6 +105,7 @@ struct DevPtrs {
   const double* newT;            // conditions for the next interval (per replica)
   const double* newP;
   const int* changed;            // 1 = apply the exchange tail at the interval start
+  int tile0;                     // first tile of a launch over a tile range (order == NULL)
 };
 
 enum : int { kErrNbrOverflow = 1, kErrNonFinite = 2, kErrHistRange = 4 };

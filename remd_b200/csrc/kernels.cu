@@ -158,7 +158,8 @@ template <bool MID>
 __global__ void __launch_bounds__(128, 7) k_integrate(DevPtrs d, const RepState* __restrict__ X,
                                                    RepState* __restrict__ Y, int prec) {
   __shared__ StepCoef sc;
-  const Tile t = d.tiles[blockIdx.x];
+  const int tix = d.tile0 + blockIdx.x;   // this launch's tile range
+  const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
   P2Sum e;
   if (threadIdx.x < 32) e = reduce_part2(d, c);
@@ -183,8 +184,8 @@ __global__ void __launch_bounds__(128, 7) k_integrate(DevPtrs d, const RepState*
       const double Li = 1.0 / st.L[x];
       sc.coef_r[x] = Li * Li * si * c.dt;
     }
-    for (int x = 0; x < 3; x++) sc.Lb[x] = d.Lbuild[3 * blockIdx.x + x];
-    if (blockIdx.x == c.tile_off) Y[t.rep] = st;
+    for (int x = 0; x < 3; x++) sc.Lb[x] = d.Lbuild[3 * tix + x];
+    if (tix == c.tile_off) Y[t.rep] = st;
   }
   __syncthreads();
   const int i = threadIdx.x;
@@ -1016,7 +1017,7 @@ template <bool FORCE_ONLY>
 __global__ void __launch_bounds__(128) k_force_f64(DevPtrs d, const RepState* __restrict__ Yin,
                                                    RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
-  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;   // costliest tiles first
+  const int tix = d.order ? d.order[blockIdx.x] : d.tile0 + blockIdx.x;   // costliest tiles first
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
   if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
@@ -1037,7 +1038,7 @@ template <bool FORCE_ONLY>
 __global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepState* __restrict__ Yin,
                                                      RepState* __restrict__ Xout, int tile_size) {
   __shared__ ForceHead h;
-  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;
+  const int tix = d.order ? d.order[blockIdx.x] : d.tile0 + blockIdx.x;
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
   if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
@@ -1060,7 +1061,7 @@ __global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepStat
 __global__ void __launch_bounds__(128, 3) k_force_pairs(DevPtrs d, const RepState* __restrict__ X,
                                                         int tile_size) {
   __shared__ double Ls[3];
-  const int tix = d.order ? d.order[blockIdx.x] : blockIdx.x;
+  const int tix = d.order ? d.order[blockIdx.x] : d.tile0 + blockIdx.x;
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
   if (threadIdx.x < 3) Ls[threadIdx.x] = X[t.rep].L[threadIdx.x];
