@@ -30,11 +30,13 @@ using namespace remd;
     }                                                                              \
   } while (0)
 
+constexpr int kMaxChains = 4;   // independent chains of the interval graph
+
 struct remd_engine_s {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t stream2 = nullptr;      // second chain of the interval graph
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t stream2[kMaxChains - 1] = {};   // further chains of the interval graph
+  cudaEvent_t ev_fork = nullptr, ev_join[kMaxChains - 1] = {};
   int prec = kF32;
   int tile = 128;
   double skin = 1.0;
@@ -44,8 +46,9 @@ struct remd_engine_s {
   std::vector<RepConst> rc;
   std::vector<Tile> tiles;
   std::vector<int> order;          // force blocks -> tiles, costliest first
-  std::vector<int> order2;         // the same per half: tiles [0, split_tile), then the rest
-  int split_tile = 0;              // 0: the interval graph runs one chain
+  std::vector<int> order2;         // the same per chain: chain k's tiles [chain_tile[k], chain_tile[k+1])
+  int nchain = 1;                  // independent chains of the interval graph
+  int chain_tile[kMaxChains + 1] = {};
   int* d_order2 = nullptr;
   std::vector<double> curT, curP;
   std::vector<double> wall_h;
@@ -167,26 +170,31 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
     h->order.resize(h->tiles.size());
     for (size_t t = 0; t < h->order.size(); t++) h->order[t] = (int)t;
     std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    // two halves of the replicas (split at the replica boundary nearest half the
-    // cost) for the two independent chains of the interval graph
-    h->split_tile = 0;
-    if (h->nrep >= 2) {
-      double tot = 0.0, run = 0.0;
-      for (double x : cost) tot += x;
-      int best = 0;
-      double bestd = 1e300;
-      for (int r = 1; r < h->nrep; r++) {
-        const RepConst& pc = h->rc[r - 1];
-        for (int t = pc.tile_off; t < pc.tile_off + pc.ntile; t++) run += cost[t];
-        const double dd = std::fabs(run - 0.5 * tot);
-        if (dd < bestd) { bestd = dd; best = h->rc[r].tile_off; }
-      }
-      h->split_tile = best;
+    // groups of whole replicas of about equal cost (boundaries at the replica
+    // boundaries nearest k/K of the total) for the independent chains of the
+    // interval graph
+    const int K = std::min(kMaxChains, h->nrep);
+    std::vector<double> before(h->nrep + 1, 0.0);   // cost of replicas [0, r)
+    for (int r = 0; r < h->nrep; r++) {
+      double w = 0.0;
+      for (int t = h->rc[r].tile_off; t < h->rc[r].tile_off + h->rc[r].ntile; t++) w += cost[t];
+      before[r + 1] = before[r] + w;
     }
+    std::vector<int> cut(1, 0);   // first replica of each chain
+    for (int k = 1; k < K; k++) {
+      const double goal = before[h->nrep] * k / K;
+      int best = cut.back() + 1;
+      for (int r = cut.back() + 1; r <= h->nrep - (K - k); r++)
+        if (std::fabs(before[r] - goal) < std::fabs(before[best] - goal)) best = r;
+      cut.push_back(best);
+    }
+    h->nchain = K;
+    for (int k = 0; k < K; k++) h->chain_tile[k] = h->rc[cut[k]].tile_off;
+    h->chain_tile[K] = (int)h->tiles.size();
     h->order2.clear();
-    for (int half = 0; half < 2; half++)
+    for (int k = 0; k < K; k++)
       for (int t : h->order)
-        if ((t < h->split_tile) == (half == 0)) h->order2.push_back(t);
+        if (t >= h->chain_tile[k] && t < h->chain_tile[k + 1]) h->order2.push_back(t);
   }
   const size_t N = h->N, nt = h->tiles.size(), nr = h->nrep;
   const size_t elem = (h->prec == kF32) ? 4 : 8;
@@ -355,27 +363,30 @@ static remd_status build_graph(remd_engine_s* h) {
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   launch_replica_start(h->d, h->X, h->stream);
-  if (h->split_tile > 0 && !h->vscale) {
-    // two independent chains, one per half of the replicas (no data crosses
-    // between them), so one half's latency-bound phases -- the integrate
-    // kernel's scalar chains, the list kernel's heads, the pair kernel's tail
-    // -- overlap the other half's work
-    DevPtrs dA = h->d, dB = h->d;
-    dA.ntiles = h->split_tile;
-    dA.order = h->d_order2;
-    dB.ntiles = h->d.ntiles - h->split_tile;
-    dB.order = h->d_order2 + h->split_tile;
-    dB.tile0 = h->split_tile;
-    cudaEventRecord(h->ev_fork, h->stream);
-    cudaStreamWaitEvent(h->stream2, h->ev_fork, 0);
-    for (int s = 0; s < h->interval; s++) {
-      launch_integrate_prec(dA, h->X, h->Y, s > 0, h->tile, h->prec, h->stream);
-      launch_force(dA, h->Y, h->X, h->prec, false, h->tile, h->stream);
-      launch_integrate_prec(dB, h->X, h->Y, s > 0, h->tile, h->prec, h->stream2);
-      launch_force(dB, h->Y, h->X, h->prec, false, h->tile, h->stream2);
+  if (h->nchain > 1 && !h->vscale) {
+    // independent chains, one per group of replicas (no data crosses between
+    // them), so one group's latency-bound phases -- the integrate kernel's
+    // scalar chains, the list kernel's heads, the pair kernel's tail -- overlap
+    // the other groups' work
+    DevPtrs dg[kMaxChains];
+    for (int k = 0; k < h->nchain; k++) {
+      dg[k] = h->d;
+      dg[k].ntiles = h->chain_tile[k + 1] - h->chain_tile[k];
+      dg[k].order = h->d_order2 + h->chain_tile[k];
+      dg[k].tile0 = h->chain_tile[k];
     }
-    cudaEventRecord(h->ev_join, h->stream2);
-    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    cudaEventRecord(h->ev_fork, h->stream);
+    for (int k = 1; k < h->nchain; k++) cudaStreamWaitEvent(h->stream2[k - 1], h->ev_fork, 0);
+    for (int s = 0; s < h->interval; s++)
+      for (int k = 0; k < h->nchain; k++) {
+        cudaStream_t st = k ? h->stream2[k - 1] : h->stream;
+        launch_integrate_prec(dg[k], h->X, h->Y, s > 0, h->tile, h->prec, st);
+        launch_force(dg[k], h->Y, h->X, h->prec, false, h->tile, st);
+      }
+    for (int k = 1; k < h->nchain; k++) {
+      cudaEventRecord(h->ev_join[k - 1], h->stream2[k - 1]);
+      cudaStreamWaitEvent(h->stream, h->ev_join[k - 1], 0);
+    }
   } else {
     for (int s = 0; s < h->interval; s++) {
       launch_step_integrate(h, s);
@@ -605,14 +616,19 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   h->nrep = rep;
   h->N = mol;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
       force_kernel_setup() != cudaSuccess) {
     set_error("cannot set up device/stream");
     delete h;
     return REMD_ERR_CUDA;
   }
+  for (int k = 0; k < kMaxChains - 1; k++)
+    if (cudaStreamCreateWithFlags(&h->stream2[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("cannot create the interval graph's streams");
+      remd_destroy(h);
+      return REMD_ERR_CUDA;
+    }
   remd_status st = allocate(h);
   if (st != REMD_OK) { remd_destroy(h); return st; }
   // host SoA staging
@@ -672,8 +688,10 @@ remd_status remd_destroy(remd_handle h) {
   if (h->d_hist) cudaFree(h->d_hist);
   if (h->d_hidx) cudaFree(h->d_hidx);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-  if (h->ev_join) cudaEventDestroy(h->ev_join);
-  if (h->stream2) cudaStreamDestroy(h->stream2);
+  for (int k = 0; k < kMaxChains - 1; k++) {
+    if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
+    if (h->stream2[k]) cudaStreamDestroy(h->stream2[k]);
+  }
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return REMD_OK;
@@ -915,9 +933,9 @@ int remd_launches_per_interval(remd_handle h) {
   // with velocity scaling also the rescale and, after the first step, the closing kick)
   // + replica_end + the device exchange when enabled (and the histogram before it)
   if (!h) return 0;
-  // (the two-chain graph, without velocity scaling, launches each step kernel once per half)
-  const bool split = h->split_tile > 0 && !h->vscale;
-  const int per_step = ((h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0)) * (split ? 2 : 1);
+  // (the multi-chain graph, without velocity scaling, launches each step kernel once per chain)
+  const int chains = h->vscale ? 1 : h->nchain;
+  const int per_step = ((h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0)) * chains;
   return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0) +
          (h->exch_enabled && h->hist_on ? 1 : 0);
 }
