@@ -11,7 +11,9 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import shutil
 import subprocess
+import tempfile
 
 import numpy as np
 
@@ -389,7 +391,7 @@ def reference_available(variant="generic"):
 
 def _ref_path(variant):
     name = {"generic": "libremdref.so", "tuned4": "libremdref_tuned4.so",
-            "shipped": "libremdref_shipped.so"}[variant]
+            "shipped": "libremdref_shipped.so", "slitwall": "libremdref_slitwall.so"}[variant]
     return os.path.join(REF_DIR, name)
 
 
@@ -431,7 +433,15 @@ class Reference:
     def __init__(self, spec: SystemSpec, state: ReplicaState, moltype_path, variant="generic"):
         lib = _ref_lib(variant)
         self.lib, self.spec = lib, spec
-        self.h = C.c_void_p(lib.ref_create(spec.inp_text(moltype_path).encode()))
+        # the reference's slit wall table is also written to ./force.dat
+        # (src/force_calculator.cxx:164): build it in a scratch directory
+        cwd, tmp = os.getcwd(), tempfile.mkdtemp()
+        try:
+            os.chdir(tmp)
+            self.h = C.c_void_p(lib.ref_create(spec.inp_text(moltype_path).encode()))
+        finally:
+            os.chdir(cwd)
+            shutil.rmtree(tmp, ignore_errors=True)
         st = state
         lib.ref_set_state(self.h, _ptr(np.ascontiguousarray(st.r, float)),
                           _ptr(np.ascontiguousarray(st.v, float)),

@@ -17,6 +17,9 @@ CASES = {
     "tip3p_tube_npz": ("tip3p", 1, 2, 1, 72, 106),
     "tip4p_bulk_vscale": ("tip4p", 0, 0, 2, 64, 107),
     "tip3p_tube_npz_vscale": ("tip3p", 1, 2, 2, 72, 108),
+    "tip4p_slit_nvt": ("tip4p", 2, 0, 1, 96, 109),
+    "tip3p_slit_nve": ("tip3p", 2, 0, 0, 80, 110),
+    "tip5p_slit_nvt": ("tip5p", 2, 0, 1, 72, 111),
 }
 NSTEPS = 20
 

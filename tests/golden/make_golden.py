@@ -13,7 +13,11 @@ Writes, next to this script:
   ref_<case>.npz       for small seeded systems: the initial state and the
                        reference's own outputs (compiled reference CPU code,
                        generic FP64 build) after InitializeProperty (a force
-                       snapshot) and after 20 MD steps.
+                       snapshot) and after 20 MD steps.  Slit systems
+                       (confined=2) use the build whose broken CPU slit wall
+                       is replaced by the reference GPU kernel's lookup
+                       (oracle/ref_slit_wall.cxx); everything else there is
+                       the reference's own code.
 The tests compare the C oracle, and through it the CUDA engine, with these.
 """
 import json
@@ -42,6 +46,9 @@ CASES = {
     "tip3p_tube_npz": ("tip3p", 1, 2, 1, 72, 106),
     "tip4p_bulk_vscale": ("tip4p", 0, 0, 2, 64, 107),
     "tip3p_tube_npz_vscale": ("tip3p", 1, 2, 2, 72, 108),
+    "tip4p_slit_nvt": ("tip4p", 2, 0, 1, 96, 109),
+    "tip3p_slit_nve": ("tip3p", 2, 0, 0, 80, 110),
+    "tip5p_slit_nvt": ("tip5p", 2, 0, 1, 72, 111),
 }
 NSTEPS = 20
 
@@ -108,7 +115,10 @@ def main():
     for name in (sys.argv[1:] or CASES):
         ens = case_ensemble(name)
         spec, st = ens.spec, ens.states[0]
-        ref = O.Reference(spec, st, spec.moltype_file)
+        # slit systems: the build whose CPU slit wall is the reference GPU kernel's
+        # (oracle/ref_slit_wall.cxx); the reference's own CPU slit branch is broken
+        variant = "slitwall" if spec.confined == 2 else "generic"
+        ref = O.Reference(spec, st, spec.moltype_file, variant=variant)
         ref.initialize_property()
         snap = ref_outputs(ref, spec)
         ref.execute_steps(NSTEPS)

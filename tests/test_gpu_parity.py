@@ -109,6 +109,35 @@ def test_twenty_steps(name, prec):
     assert eng.replica_status(0) == 0
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_fp64_engine_matches_reference_fixtures(name):
+    """The FP64 engine against the reference's own outputs (tests/golden/ref_*.npz,
+    compiled reference CPU code; slit systems from the build whose CPU slit wall is
+    the reference GPU kernel's lookup): the force snapshot at the oracle's bounds and
+    20 MD steps at the trajectory bounds."""
+    spec, st, z = load_case(name)
+    eng = E.REMDGPU([single(spec, st)], precision="fp64", interval=NSTEPS)
+    g = eng.ConvertVariablesToHost(0)
+    assert rel(g["f"], z["snap_f"]) < 1e-10
+    assert rel(g["n"], z["snap_n"]) < 1e-10
+    e = z["snap_ener"]
+    scale = abs(e[0]) + abs(e[1]) + abs(e[2])
+    assert g["lj"] == pytest.approx(e[0], abs=1e-11 * scale)
+    assert g["clmb"] == pytest.approx(e[1], abs=1e-11 * scale)
+    assert g["wall"] == pytest.approx(e[2], abs=1e-11 * scale)
+    assert rel(g["vir"], e[3:6]) < 1e-10
+    eng.ExecuteSteps(np.array([st.T]), np.array([st.P]))
+    g = eng.ConvertVariablesToHost(0)
+    assert rel(g["r"], z["after_r"]) < 1e-9
+    assert rel(g["q"], z["after_q"]) < 1e-8
+    assert rel(g["v"], z["after_v"]) < 1e-7
+    assert rel(g["p"], z["after_p"]) < 1e-7
+    sc = z["after_scal"]
+    assert g["s"] == pytest.approx(sc[0], rel=1e-9)
+    assert np.allclose(g["L"], sc[5:8], rtol=1e-12)
+    eng.close()
+
+
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 def test_condition_change_applies_exchange_tail(prec):
     """ExecuteSteps with a new (T,P) runs ChangeTemperature, KillMomentum,
@@ -360,6 +389,25 @@ def test_fp32_accuracy_large_systems(model, confined, wall, rc):
     assert rel(g["n"], orc.n) < 1e-5
     assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
     assert abs(eng.pair_count() - orc.prop()["npairs"]) <= 2
+    eng.close()
+
+
+@pytest.mark.parametrize("wall", [4.5, 5.0])
+def test_fp32_accuracy_narrow_tube(wall):
+    """Single-file water in the narrowest tubes of the batch's radius range
+    (4.5 and 5 A, 256 TIP4P molecules on a 768 A axis): the FP32 gates hold where
+    the wall term is as large as the pair terms."""
+    e = S.make_ensemble("nt", "tip4p", 1, 256, wall, 8.5, 7.5, 1, 1, 300, 300, 0.1e6, 0.1e6, 45)
+    st = e.states[0]
+    eng = E.REMDGPU([single(e.spec, st)], precision="fp32")
+    g = eng.ConvertVariablesToHost(0)
+    orc = O.Oracle(e.spec, st)
+    orc.initialize_property()
+    assert rel(g["f"], orc.f) < 1e-5
+    assert rel(g["n"], orc.n) < 1e-5
+    assert g["pot"] == pytest.approx(orc.prop()["pot"], rel=1e-6)
+    assert g["wall"] == pytest.approx(orc.prop()["wall"], rel=1e-6)
+    assert eng.pair_count() == orc.prop()["npairs"]
     eng.close()
 
 

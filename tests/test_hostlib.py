@@ -46,13 +46,22 @@ def test_wall_table_bitwise_equal_to_oracle(confined, nfwall, wall):
     assert np.array_equal(a, b)
 
 
-def test_wall_table_matches_reference_object():
+@pytest.mark.parametrize("case,nfwall,wall", [("tip4p_tube_npz", None, None), ("tip4p_slit_nvt", None, None),
+                                               ("tip3p_slit_nve", 500, 7.3), ("tip5p_slit_nvt", 4096, 14.0)])
+def test_wall_table_matches_reference_object(case, nfwall, wall):
+    """The table the engine builds equals ForceCalculator::fwall of the
+    reference's own object (src/force_calculator.cxx:117-200), bit for bit,
+    for the nanotube and for the nano-slit (confined=2, 163-199)."""
     if not O.reference_available():
         pytest.skip("oracle/_ref not built")
+    import dataclasses
     from tests.common import load_case
-    spec, st, _ = load_case("tip4p_tube_npz")
+    spec, st, _ = load_case(case)
+    if nfwall is not None:
+        spec = dataclasses.replace(spec, nfwall=nfwall, wall_length=wall)
     ref = O.Reference(spec, st, spec.moltype_file)
-    t = E.wall_table(1, spec.nfwall, spec.wall_length, spec.sgm_wall, spec.eps_wall, spec.rho_wall)
+    t = E.wall_table(spec.confined, spec.nfwall, spec.wall_length, spec.sgm_wall, spec.eps_wall,
+                     spec.rho_wall)
     assert np.array_equal(t, ref.fwall())
 
 
