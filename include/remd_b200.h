@@ -255,8 +255,24 @@ remd_status remd_wall_table(int confined, int nfwall, double wall_length, double
  * reference; scal = s Ps Q Pv0 Pv1 Pv2 W L0 L1 L2). */
 remd_status remd_read_chk(const char *path, int nmol, double *r, double *v, double *q, double *p,
                           double *mass, double *inertia, double *scal);
-/* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) of replica rep. */
+/* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) of replica rep, with
+ * the reference's text layout byte for byte.  The last line is the replica's
+ * Property (src/variables.h:51-74) as the engine holds it after the last call:
+ * time = MD steps run by the handle x dt, the energies and pressures of the
+ * last interval's averages (or of the initial force call), the momentum and the
+ * virial of the current state; the running averages Tave and Pave are those of
+ * the last property evaluation alone (the reference's nave = 1). */
 remd_status remd_write_chk(remd_handle h, int rep, const char *path);
+/* IOManager::WriteCheckPoint (src/io_manager.cxx:593-634) from host arrays in the
+ * remd_read_chk convention (r box fraction, v * L * s, p * s, nmol rows each;
+ * mass and inertia[3], the principal moments, shared by every molecule;
+ * scal = s Ps Q Pv0 Pv1 Pv2 W L0 L1 L2).
+ * prop holds the 26 numbers of the Property line in its operator<< order
+ * (src/variables.h:51-74): time pot tra rot kin tsm tsp tst bst tot ham, tmo[3],
+ * Tave/nave, prs[4], vir[3], Pave[4]/nave. */
+remd_status remd_write_chk_arrays(const char *path, int nmol, int nsite, const double *r,
+                                  const double *v, const double *q, const double *p, double mass,
+                                  const double *inertia, const double *scal, const double *prop);
 /* The .gro output of replica rep as IOManager::UpdateOutputs writes it
  * (src/io_manager.cxx:636-651 -> ConvertMoleculesToAtoms 797-814 ->
  * write_gro_file, src/gro.cxx:118-135): comment "test", site coordinates
@@ -311,9 +327,14 @@ remd_status remd_histogram_read(remd_handle h, int ens, const char *dir);
  * REMD_PREC_FP32 handle's remd_compute_forces.  All working memory is one
  * fixed device array of the library (about 8.8 MB, held by every GPU that
  * loads it until exit): at most 2048 molecules and 1024 neighbours per molecule
- * (rcut <= ~12.4 A); larger inputs are rejected with REMD_ERR_INVALID.  The
- * first call on a device looks up that array's device address (set-up), so make
- * it before any stream capture.  Calls share the array and keep the previous
+ * (rcut <= ~12.4 A); larger inputs are rejected with REMD_ERR_INVALID, and so
+ * are a d_wall that is not 16-byte aligned and other buffers that are not
+ * 8-byte aligned.  The first call on a device looks up that array's device
+ * address (set-up) and keeps it for the process, so make it before any stream
+ * capture, and make no call after a cudaDeviceReset of that device (the reset
+ * reloads the library's module, and the kept address may no longer be the
+ * array's).  The constants of a call travel as kernel parameters, so no host
+ * buffer has to outlive the call.  Calls share the array and keep the previous
  * call's contents, so calls that overlap on the GPU (other streams, other
  * threads) race; serialise them.  Asynchronous on `stream` (a cudaStream_t,
  * NULL = default stream). */

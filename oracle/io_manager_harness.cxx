@@ -16,12 +16,6 @@
 #include "io_manager.h"
 #include "remd_b200.h"
 
-namespace remd {
-int write_chk(const char* path, int nmol, int nsite, const double* r, const double* v,
-              const double* q, const double* p, double mass, const double* I, double s, double Ps,
-              double Q, const double* Pv, double W, const double* L);
-}
-
 // File names as InputParam(const Parameter) forms them (src/io_manager.cxx:88-156):
 // prefix + name + extension, "null" kept as is; the checkpoint output name has
 // no extension here (WriteCheckPoint appends the replica index and ".chk").
@@ -98,10 +92,10 @@ void IOManager::ReadInputs(Molecule* m, Thermostat* tst, Barostat* bst, MolTypeL
   bst->W = sc[6];
 }
 
-// WriteCheckPoint (src/io_manager.cxx:593-634) through the engine's .chk writer.
+// WriteCheckPoint (src/io_manager.cxx:593-634) through the engine's .chk writer
+// (remd_write_chk_arrays), with the caller's Property on the last line.
 void IOManager::WriteCheckPoint(const Molecule* m, const Thermostat* tst, const Barostat* bst,
                                 const dvec3 L, const Property prop, const int index) {
-  (void)prop;
   char path[300];
   std::snprintf(path, sizeof(path), "%s%04d.chk", iprm->ochk, index);
   std::vector<double> r(3 * nmol), v(3 * nmol), q(4 * nmol), p(4 * nmol);
@@ -110,11 +104,18 @@ void IOManager::WriteCheckPoint(const Molecule* m, const Thermostat* tst, const 
     for (int x = 0; x < 4; x++) { q[4 * i + x] = m[i].q[x]; p[4 * i + x] = m[i].p[x]; }
   }
   const double I[3] = {m[0].i[0], m[0].i[1], m[0].i[2]};
-  const double Pv[3] = {bst->Pv[0], bst->Pv[1], bst->Pv[2]};
-  const double LL[3] = {L[0], L[1], L[2]};
+  const double scal[10] = {tst->s, tst->Ps, tst->Q, bst->Pv[0], bst->Pv[1], bst->Pv[2], bst->W,
+                           L[0], L[1], L[2]};
   const int nsite = natom / nmol;
-  if (remd::write_chk(path, nmol, nsite, r.data(), v.data(), q.data(), p.data(), m[0].m, I, tst->s,
-                      tst->Ps, tst->Q, Pv, bst->W, LL) != REMD_OK) {
+  // the caller's Property, as the reference's operator<< prints it (src/variables.h:51-74)
+  const double nave = (prop.nave != 0) ? (double)prop.nave : 1.0;
+  const double pv[26] = {
+      prop.time, prop.pot, prop.tra, prop.rot, prop.kin, prop.tsm, prop.tsp, prop.tst, prop.bst,
+      prop.tot, prop.ham, prop.tmo[0], prop.tmo[1], prop.tmo[2], prop.Tave / nave,
+      prop.prs[0], prop.prs[1], prop.prs[2], prop.prs[3], prop.vir[0], prop.vir[1], prop.vir[2],
+      prop.Pave[0] / nave, prop.Pave[1] / nave, prop.Pave[2] / nave, prop.Pave[3] / nave};
+  if (remd_write_chk_arrays(path, nmol, nsite, r.data(), v.data(), q.data(), p.data(), m[0].m, I, scal,
+                            pv) != REMD_OK) {
     std::fprintf(stderr, "io_manager_harness: %s\n", remd_last_error());
     std::exit(EXIT_FAILURE);
   }

@@ -420,8 +420,9 @@ def _ref_lib(variant="generic"):
         lib.ref_remdinfo_read_histogram.argtypes = [C.c_void_p]
         lib.ref_write_gro.argtypes = [C.c_char_p, C.c_int, _ip, C.POINTER(C.c_char_p),
                                       C.POINTER(C.c_char_p), _ip, _dp, _dp, C.c_char_p]
+        lib.ref_write_chk.argtypes = [C.c_void_p, C.c_char_p]
         for fn in ["ref_set_state", "ref_get_state", "ref_get_property", "ref_get_average",
-                   "ref_get_fwall"]:
+                   "ref_get_fwall", "ref_get_property_line"]:
             getattr(lib, fn).argtypes = None
         _REFLIBS[variant] = lib
     return _REFLIBS[variant]
@@ -481,6 +482,14 @@ class Reference:
         o = np.zeros(NUM_AVG)
         self.lib.ref_get_average(self.h, _ptr(o))
         return o
+
+    def property_line(self):
+        o = np.zeros(26)
+        self.lib.ref_get_property_line(self.h, _ptr(o))
+        return o
+
+    def write_chk(self, path):
+        self.lib.ref_write_chk(self.h, path.encode())
 
     def fwall(self):
         o = np.zeros(2 * self.spec.nfwall)

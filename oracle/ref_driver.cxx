@@ -15,6 +15,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -113,6 +114,43 @@ void ref_get_property(void* hp, double* out) {
                          pr.tra,   pr.rot,    pr.kin,    pr.T,      pr.prs[0], pr.prs[1], pr.prs[2],
                          pr.prs[3], pr.tst,   pr.bst,    pr.tot,    pr.ham,    pr.H0,     pr.gkT};
   std::memcpy(out, vals, sizeof(vals));
+}
+
+// The 26 numbers of the .chk Property line, in operator<< order (src/variables.h:51-74).
+void ref_get_property_line(void* hp, double* out) {
+  const Property& p = static_cast<RefHandle*>(hp)->m->prop;
+  const double nave = (p.nave != 0) ? (double)p.nave : 1.0;
+  const double v[26] = {p.time, p.pot, p.tra, p.rot, p.kin, p.tsm, p.tsp, p.tst, p.bst, p.tot, p.ham,
+                        p.tmo[0], p.tmo[1], p.tmo[2], p.nave != 0 ? p.Tave / nave : p.Tave,
+                        p.prs[0], p.prs[1], p.prs[2], p.prs[3], p.vir[0], p.vir[1], p.vir[2],
+                        p.Pave[0] / nave, p.Pave[1] / nave, p.Pave[2] / nave, p.Pave[3] / nave};
+  std::memcpy(out, v, sizeof(v));
+}
+
+// A .chk of the object's state written with the stream statements of
+// IOManager::WriteCheckPoint (src/io_manager.cxx:611-632) and the reference's
+// own operator<< for Vector (src/vector.h:141-147) and Property
+// (src/variables.h:51-74).  io_manager.cxx itself cannot be compiled here.
+void ref_write_chk(void* hp, const char* path) {
+  Molecules* m = static_cast<RefHandle*>(hp)->m;
+  std::ofstream ofs(path, std::ios_base::out);
+  ofs << m->nmol << " " << m->natom << std::endl;
+  for (int i = 0; i < m->nmol; i++) {
+    const Molecule& a = m->mlcl[i];
+    ofs << a.r * m->L;
+    ofs << a.v / (m->L * m->tst->s);
+    ofs << a.q;
+    ofs << a.p / m->tst->s;
+    ofs << " " << a.m;
+    ofs << " " << a.i;
+    ofs << " " << a.type;
+    ofs << " " << a.id;
+    ofs << std::endl;
+  }
+  ofs << m->tst->s << " " << m->tst->Ps << " " << m->tst->Q << std::endl;
+  ofs << m->bst->Pv << " " << m->bst->W << std::endl;
+  ofs << m->L << std::endl;
+  ofs << m->prop << std::endl;
 }
 
 void ref_get_average(void* hp, double* out) {

@@ -71,6 +71,7 @@ struct remd_engine_s {
   long long* d_step = nullptr;      // per-ensemble interval counter of the device exchange
   unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
   long long last_pairs = 0;
+  long long steps_done = 0;        // MD steps run (the simulated time of the .chk Property line)
   size_t bytes = 0;
   // (volume, potential) histograms per condition slot, per ensemble (own allocations)
   std::vector<HistEns> hist;        // host copy of d_hist (device pointers inside)
@@ -302,10 +303,15 @@ static remd_status allocate(remd_engine_s* h) {
   return REMD_OK;
 }
 
+// Waits for the handle's stream and reports the device error word.  The word
+// is cleared once read, so an error is reported by the call whose work raised
+// it and a later call starts clean (a replica that stays non-finite raises it
+// again; its per-replica status word keeps the cause).
 static remd_status sync_and_check(remd_engine_s* h) {
   CK(cudaStreamSynchronize(h->stream));
   int err = 0;
   CK(cudaMemcpy(&err, h->d.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err != 0) CK(cudaMemset(h->d.err, 0, sizeof(int)));
   if (err & kErrNbrOverflow) {
     set_error("neighbour list capacity exceeded");
     return REMD_ERR_NEIGHBOR_OVERFLOW;
@@ -779,6 +785,7 @@ remd_status remd_autotune(remd_handle h, int nsteps, int* tile_out, double* skin
   SavedState sv;
   remd_status s = save_state(h, sv);
   if (s != REMD_OK) return s;
+  const long long steps0 = h->steps_done;   // the trials' steps are undone with the state
   static const int tiles[] = {32, 64, 96, 128};
   static const double skins[] = {0.2, 0.4, 0.6, 0.8, 1.0, 1.4};
   int best_tile = h->tile;
@@ -793,6 +800,7 @@ remd_status remd_autotune(remd_handle h, int nsteps, int* tile_out, double* skin
       if (step_ms < best_ms) { best_ms = step_ms; best_tile = t; best_skin = k; }
     }
   if ((s = relayout(h, best_tile, best_skin, sv)) != REMD_OK) return s;
+  h->steps_done = steps0;
   if (tile_out) *tile_out = best_tile;
   if (skin_out) *skin_out = best_skin;
   if (ms_out) *ms_out = best_ms;
@@ -816,6 +824,7 @@ remd_status remd_execute_steps_async(remd_handle h, const double* T, const doubl
     if (s != REMD_OK) return s;
   }
   CK(cudaGraphLaunch(h->gexec, h->stream));
+  h->steps_done += h->interval;
   return REMD_OK;
 }
 
@@ -850,6 +859,7 @@ remd_status remd_execute_nsteps(remd_handle h, int nsteps) {
   }
   launch_replica_end(h->d, h->X, h->stream);
   CK(cudaGetLastError());
+  h->steps_done += nsteps;
   return sync_and_check(h);
 }
 
@@ -974,6 +984,7 @@ remd_status remd_profile_steps(remd_handle h, int nsteps, double* ms_out) {
   }
   launch_replica_end(h->d, h->X, h->stream);
   for (auto& e : ev) cudaEventDestroy(e);
+  h->steps_done += nsteps;
   ms_out[0] = ti / nsteps;
   ms_out[1] = tf / nsteps;
   return sync_and_check(h);
@@ -1071,8 +1082,37 @@ remd_status remd_write_chk(remd_handle h, int rep, const char* path) {
   o.r = r.data(); o.v = v.data(); o.q = q.data(); o.p = p.data();
   remd_status s = remd_get_state(h, rep, &o);
   if (s != REMD_OK) return s;
+  double a[kNumAvg];
+  if ((s = remd_get_averages(h, rep, a)) != REMD_OK) return s;
+  // the Property line (Molecules::CalcProperties, src/molecules.cxx:702-734)
+  double prop[kChkPropCount];
+  double t = 0.0;   // prop.time += unit_time * dt once per MD step (src/integrator.cxx:795)
+  for (long long k = 0; k < h->steps_done; k++) t += unit_time() * c.dt;
+  const double gkT = 6.0 * (double)n * o.T;
+  const double tsm = 0.5 * o.Ps * o.Ps / o.Q, tsp = gkT * std::log(o.s);
+  double bst = 0.0;   // Molecules::BarostatEnergy (src/molecules.cxx:663-678); slit: GPU form
+  if (c.pconstant > 0) {
+    if (c.confined == 0)
+      bst = 0.5 * (o.Pv[0] * o.Pv[0] + o.Pv[1] * o.Pv[1] + o.Pv[2] * o.Pv[2]) / c.W + o.P * o.L[0] * o.L[1] * o.L[2];
+    else if (c.confined == 1)
+      bst = 0.5 * o.Pv[2] * o.Pv[2] / c.W + o.P * (c.bottom_area * o.L[2]);
+    else
+      bst = (o.Pv[0] * o.Pv[0] + o.Pv[1] * o.Pv[1]) * (0.5 / c.W) + o.P * (o.L[0] * o.L[1] * c.slit_width);
+  }
+  double tmo[3] = {0.0, 0.0, 0.0};   // Molecules::Momentum (src/molecules.cxx:679-686)
+  for (int x = 0; x < 3; x++) {
+    const double cf = 1.0 / (o.L[x] * o.s);
+    for (int i = 0; i < n; i++) tmo[x] += v[3 * i + x] * c.mass * cf;
+  }
+  const double up = unit_press();
+  const double prs[4] = {a[REMD_AVG_PX] * up, a[REMD_AVG_PY] * up, a[REMD_AVG_PZ] * up, a[REMD_AVG_P] * up};
+  const double vals[kChkPropCount] = {
+      t, a[0] + a[1] + a[2], a[REMD_AVG_TRA], a[REMD_AVG_ROT], a[REMD_AVG_TRA] + a[REMD_AVG_ROT], tsm, tsp,
+      tsm + tsp, bst, a[REMD_AVG_TOT], a[REMD_AVG_DRF], tmo[0], tmo[1], tmo[2], a[REMD_AVG_T] * unit_temp(),
+      prs[0], prs[1], prs[2], prs[3], o.vir[0], o.vir[1], o.vir[2], prs[0], prs[1], prs[2], prs[3]};
+  std::memcpy(prop, vals, sizeof(prop));
   return (remd_status)write_chk(path, n, c.nsite, r.data(), v.data(), q.data(), p.data(), c.mass, c.I,
-                                o.s, o.Ps, o.Q, o.Pv, o.W, o.L);
+                                o.s, o.Ps, o.Q, o.Pv, o.W, o.L, prop);
 }
 
 remd_status remd_write_gro(remd_handle h, int rep, const char* path, const char* mol_name,

@@ -187,9 +187,18 @@ int read_chk(const char* path, int nmol, double* r, double* v, double* q, double
   return REMD_OK;
 }
 
+// The stream formats of the reference: Vector's operator<< writes ' ' then each
+// component in std::scientific (src/vector.h:141-147), which stays in effect for
+// the scalars after it; Property's operator<< writes its first eleven scalars
+// with std::setw(10) (no padding for a finite %e, 12+ characters), each followed
+// by ' ', then Vector and scalar fields each followed by ' ' (src/variables.h:51-74).
 int write_chk(const char* path, int nmol, int nsite, const double* r, const double* v,
               const double* q, const double* p, double mass, const double* I, double s, double Ps,
-              double Q, const double* Pv, double W, const double* L) {
+              double Q, const double* Pv, double W, const double* L, const double* prop) {
+  if (!prop) {
+    set_error("chk: the Property line's values are missing");
+    return REMD_ERR_INVALID;
+  }
   FILE* f = std::fopen(path, "w");
   if (!f) {
     set_error(std::string("cannot write ") + path);
@@ -213,7 +222,20 @@ int write_chk(const char* path, int nmol, int nsite, const double* r, const doub
   std::fprintf(f, "%e %e %e\n", s, Ps, Q);
   std::fprintf(f, " %e %e %e %e\n", Pv[0], Pv[1], Pv[2], W);
   std::fprintf(f, " %e %e %e\n", L[0], L[1], L[2]);
-  std::fclose(f);
+  // the Property line: time ... ham, tmo, Tave, prs, vir, Pave
+  for (int k = 0; k < 11; k++) std::fprintf(f, "%10e ", prop[k]);
+  for (int k = 11; k < 14; k++) std::fprintf(f, " %e", prop[k]);
+  std::fprintf(f, " %e ", prop[14]);
+  for (int k = 15; k < 19; k++) std::fprintf(f, " %e", prop[k]);
+  std::fprintf(f, " ");
+  for (int k = 19; k < 22; k++) std::fprintf(f, " %e", prop[k]);
+  std::fprintf(f, " ");
+  for (int k = 22; k < 26; k++) std::fprintf(f, " %e", prop[k]);
+  std::fprintf(f, " \n");
+  if (std::fclose(f) != 0) {
+    set_error(std::string("chk: write failed: ") + path);
+    return REMD_ERR_IO;
+  }
   return REMD_OK;
 }
 
@@ -254,6 +276,17 @@ remd_status remd_read_chk(const char* path, int nmol, double* r, double* v, doub
     return REMD_ERR_INVALID;
   }
   return (remd_status)remd::read_chk(path, nmol, r, v, q, p, mass, inertia, scal);
+}
+
+remd_status remd_write_chk_arrays(const char* path, int nmol, int nsite, const double* r,
+                                  const double* v, const double* q, const double* p, double mass,
+                                  const double* inertia, const double* scal, const double* prop) {
+  if (!path || nmol < 1 || nsite < 1 || !r || !v || !q || !p || !inertia || !scal || !prop) {
+    remd::set_error("remd_write_chk_arrays: bad arguments");
+    return REMD_ERR_INVALID;
+  }
+  return (remd_status)remd::write_chk(path, nmol, nsite, r, v, q, p, mass, inertia, scal[0], scal[1],
+                                      scal[2], scal + 3, scal[6], scal + 7, prop);
 }
 
 }  // extern "C"

@@ -1531,11 +1531,13 @@ int measure_fp32_fma(int device, double* ms, long long* flops) {
 // ------------------------------------------------------------------ caller-buffer variant
 // Entry and exit kernels of remd_force_snapshot_noalloc (noalloc.cu): the
 // caller's AoS positions/quaternions into the scratch SoA arrays and force
-// records, and the scratch results back into the caller's AoS outputs.
-__global__ void k_noalloc_load(DevPtrs d, const double* __restrict__ r_aos,
-                               const double* __restrict__ q_aos) {
-  const Tile t = d.tiles[blockIdx.x];
-  const RepConst& c = d.rc[t.rep];
+// records, and the scratch results back into the caller's AoS outputs.  The
+// constants, tiles and box arrive as a kernel parameter; block 0 stores them
+// into the scratch for the force kernels that follow on the same stream.
+__global__ void k_noalloc_load(DevPtrs d, const NoAllocSetup setup, RepState* __restrict__ X,
+                               const double* __restrict__ r_aos, const double* __restrict__ q_aos) {
+  const Tile t = setup.tiles[blockIdx.x];
+  const RepConst& c = setup.c;
   const int i = threadIdx.x;
   if (i < t.count) {
     const int li = t.start + i;
@@ -1550,7 +1552,13 @@ __global__ void k_noalloc_load(DevPtrs d, const double* __restrict__ r_aos,
   if (i == 0) {
     const double nan = __longlong_as_double(0x7ff8000000000000ll);
     d.Lbuild[3 * blockIdx.x] = nan;
-    if (blockIdx.x == 0) { *d.err = 0; d.status[0] = 0; }
+    if (blockIdx.x == 0) {
+      *const_cast<RepConst*>(d.rc) = setup.c;
+      for (int k = 0; k < d.ntiles; k++) const_cast<Tile*>(d.tiles)[k] = setup.tiles[k];
+      *X = setup.rs;
+      *d.err = 0;
+      d.status[0] = 0;
+    }
   }
 }
 
@@ -1576,9 +1584,9 @@ __global__ void k_noalloc_store(DevPtrs d, double* __restrict__ f_aos, double* _
   }
 }
 
-void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
-                         cudaStream_t s) {
-  k_noalloc_load<<<d.ntiles, tile, 0, s>>>(d, r_aos, q_aos);
+void launch_noalloc_load(const DevPtrs& d, const NoAllocSetup& setup, RepState* X, const double* r_aos,
+                         const double* q_aos, int tile, cudaStream_t s) {
+  k_noalloc_load<<<d.ntiles, tile, 0, s>>>(d, setup, X, r_aos, q_aos);
 }
 void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s) {
   k_noalloc_store<<<1, 256, 0, s>>>(d, f_aos, n_aos, out);

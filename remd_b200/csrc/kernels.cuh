@@ -43,8 +43,16 @@ void launch_exchange_k(const DevPtrs& d, const int* grid, const int* rep_off, co
 void launch_histogram(const DevPtrs& d, const HistEns* he, const int* rep_off, const int* index,
                       cudaStream_t s);
 int pack_stride(int nsite, int prec);
-void launch_noalloc_load(const DevPtrs& d, const double* r_aos, const double* q_aos, int tile,
-                         cudaStream_t s);
+// Set-up of one remd_force_snapshot_noalloc call, passed by value to its load
+// kernel (kernel parameters, so no host staging buffer has to outlive the call).
+constexpr int kNoAllocMaxTiles = 32;
+struct NoAllocSetup {
+  RepConst c;
+  RepState rs;
+  Tile tiles[kNoAllocMaxTiles];
+};
+void launch_noalloc_load(const DevPtrs& d, const NoAllocSetup& setup, RepState* X, const double* r_aos,
+                         const double* q_aos, int tile, cudaStream_t s);
 void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s);
 int measure_fp32_fma(int device, double* ms, long long* flops);
 

@@ -31,7 +31,7 @@ namespace {
 constexpr int kNoAllocMaxMol = 2048;
 constexpr int kNoAllocMaxNbr = 1024;
 constexpr int kNoAllocTile = 64;
-constexpr int kNoAllocMaxTiles = kNoAllocMaxMol / kNoAllocTile;
+static_assert(kNoAllocMaxTiles * kNoAllocTile == kNoAllocMaxMol, "one tile per 64 molecules");
 constexpr double kNoAllocSkin = 1.0;
 
 constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -91,6 +91,15 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
                                                    double* d_out, void* stream) {
   if (!s || !d_r || !d_q || !L || !d_f || !d_n || !d_out) {
     set_error("remd_force_snapshot_noalloc: null argument");
+    return REMD_ERR_INVALID;
+  }
+  // the kernels read d_wall as {f, U} double pairs (16-byte loads) and the
+  // other buffers as doubles
+  const auto misaligned = [](const void* p, uintptr_t a) { return ((uintptr_t)p % a) != 0; };
+  if (misaligned(d_r, 8) || misaligned(d_q, 8) || misaligned(d_f, 8) || misaligned(d_n, 8) ||
+      misaligned(d_out, 8) || (d_wall && misaligned(d_wall, 16))) {
+    set_error("remd_force_snapshot_noalloc: d_wall must be 16-byte aligned and the other buffers "
+              "8-byte aligned");
     return REMD_ERR_INVALID;
   }
   if (s->nmol < 2 || s->nmol > kNoAllocMaxMol) {
@@ -166,17 +175,17 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   c.sgm2 = sg * sg;
   const double eo = s->site_eps[0] * (1e+03 / 6.0221367e+23 / unit_energy());
   c.eps = std::sqrt(eo * eo);
-  Tile tiles[kNoAllocMaxTiles];
+  NoAllocSetup setup;
+  std::memset(&setup, 0, sizeof(setup));
+  setup.c = c;
   for (int t = 0; t < c.ntile; t++) {
-    tiles[t].rep = 0;
-    tiles[t].start = t * kNoAllocTile;
-    tiles[t].count = (s->nmol - t * kNoAllocTile < kNoAllocTile) ? s->nmol - t * kNoAllocTile : kNoAllocTile;
-    tiles[t].pad = 0;
+    setup.tiles[t].rep = 0;
+    setup.tiles[t].start = t * kNoAllocTile;
+    setup.tiles[t].count = (s->nmol - t * kNoAllocTile < kNoAllocTile) ? s->nmol - t * kNoAllocTile : kNoAllocTile;
+    setup.tiles[t].pad = 0;
   }
-  RepState rs;
-  std::memset(&rs, 0, sizeof(rs));
-  rs.s = 1.0;
-  for (int x = 0; x < 3; x++) rs.L[x] = L[x];
+  setup.rs.s = 1.0;
+  for (int x = 0; x < 3; x++) setup.rs.L[x] = L[x];
 
   DevPtrs d{};
   d.N = s->nmol;
@@ -205,15 +214,10 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   RepState* X = reinterpret_cast<RepState*>(b + kOffState);
 
   // every earlier call's contents are overwritten before use: constants, tiles
-  // and state here, records / lists / counts / partial sums by the kernels
-  // (the list validity flag is reset by the load kernel, so lists are rebuilt)
-  if (cudaMemcpyAsync(b + kOffRc, &c, sizeof(c), cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-      cudaMemcpyAsync(b + kOffTiles, tiles, sizeof(Tile) * c.ntile, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-      cudaMemcpyAsync(X, &rs, sizeof(rs), cudaMemcpyHostToDevice, cs) != cudaSuccess) {
-    set_error("remd_force_snapshot_noalloc: upload of the constants failed");
-    return REMD_ERR_CUDA;
-  }
-  launch_noalloc_load(d, d_r, d_q, kNoAllocTile, cs);
+  // and state by the load kernel (from its parameter), records / lists / counts
+  // / partial sums by the kernels after it (the load kernel also marks the lists
+  // invalid, so they are rebuilt)
+  launch_noalloc_load(d, setup, X, d_r, d_q, kNoAllocTile, cs);
   launch_force(d, X, X, kF32, true, kNoAllocTile, cs);
   launch_noalloc_store(d, d_f, d_n, d_out, cs);
   const cudaError_t e = cudaGetLastError();

@@ -205,6 +205,25 @@ static remd_status build_batch(remd_server_s* S) {
   return engine_set_exchange(S->batch, grids.data(), seeds.data(), steps.data(), index.data());
 }
 
+// The status of building job j alone (its initial force call and H0).
+static remd_status job_alone_status(remd_server_s* S, Job* j) {
+  std::vector<remd_replica_init> init;
+  for (int k = 0; k < j->nrep(); k++) {
+    const Rep& R = j->reps[k];
+    remd_replica_init ri{};
+    ri.r = R.r.data(); ri.v = R.v.data(); ri.q = R.q.data(); ri.p = R.p.data();
+    ri.mass = R.m.data(); ri.inertia = R.I.data();
+    ri.s = R.s; ri.Ps = R.Ps; ri.Q = R.Q; ri.W = R.W; ri.T = R.T; ri.P = R.P;
+    for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
+    init.push_back(ri);
+  }
+  const int per = j->nrep();
+  remd_handle h = nullptr;
+  const remd_status st = remd_create(&j->sys, 1, &per, init.data(), S->prec, S->device, &h);
+  if (h) remd_destroy(h);
+  return st;
+}
+
 extern "C" {
 
 remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision prec,
@@ -360,6 +379,27 @@ remd_status remd_server_step(remd_server S, int* pending) {
   // 3. rebuild the batch handle if its membership changed
   if (S->dirty) {
     remd_status st = build_batch(S);
+    if (st != REMD_OK && st != REMD_ERR_CUDA) {
+      // a job whose own state cannot start (e.g. a neighbour list over capacity
+      // in the initial force call) fails alone: find it by building each job
+      // that has not run yet on its own, then rebuild without the failures
+      bool any = false;
+      for (size_t e = 0; e < S->active.size();) {
+        Job* j = S->active[e];
+        const remd_status sj = j->done == 0 ? job_alone_status(S, j) : REMD_OK;
+        if (sj != REMD_OK) {
+          j->state = 3;
+          j->status = sj;
+          j->t_end = now_s() - S->t0;
+          S->in_use -= j->bytes;
+          S->active.erase(S->active.begin() + e);
+          any = true;
+        } else {
+          e++;
+        }
+      }
+      if (any) st = build_batch(S);
+    }
     if (st != REMD_OK) {
       for (Job* j : S->active) { j->state = 3; j->status = st; }
       S->active.clear();
@@ -379,13 +419,33 @@ remd_status remd_server_step(remd_server S, int* pending) {
     S->intervals_done++;
     int total = 0;
     for (Job* j : S->active) total += j->nrep();
+    // A replica that went non-finite or overflowed its neighbour list fails its
+    // own job only: the replicas of the other jobs are independent of it, their
+    // interval is complete and valid, and they keep running.
+    std::vector<char> bad(S->active.size(), 0);
+    if (st == REMD_ERR_NONFINITE || st == REMD_ERR_NEIGHBOR_OVERFLOW) {
+      int rep = 0, nbad = 0;
+      for (size_t e = 0; e < S->active.size(); e++)
+        for (int k = 0; k < S->active[e]->nrep(); k++, rep++) {
+          int w = 0;
+          if (remd_replica_status(S->batch, rep, &w) != REMD_OK) w = 1;
+          if (w != 0 && !bad[e]) { bad[e] = 1; nbad++; }
+        }
+      if (nbad > 0) {
+        for (size_t e = 0; e < S->active.size(); e++)
+          if (bad[e]) { S->active[e]->state = 3; S->active[e]->status = st; }
+        st = REMD_OK;
+      }
+    }
     std::vector<double> avg((size_t)total * 19);
     if (st == REMD_OK) st = remd_get_all_averages(S->batch, avg.data());
     int rep = 0;
     bool left = false;
-    for (Job* j : S->active) {
+    for (size_t e = 0; e < S->active.size(); e++) {
+      Job* j = S->active[e];
       j->avg.assign(avg.begin() + (size_t)rep * 19, avg.begin() + (size_t)(rep + j->nrep()) * 19);
       rep += j->nrep();
+      if (bad[e]) { left = true; continue; }
       if (st != REMD_OK) { j->state = 3; j->status = st; left = true; continue; }
       j->done++;
       S->mol_steps += (long long)j->sys.nmol * j->nrep() * j->sys.interval;

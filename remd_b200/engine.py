@@ -125,6 +125,8 @@ def lib():
         L.remd_wall_table.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                       C.c_double, _dp]
         L.remd_read_chk.argtypes = [C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.remd_write_chk_arrays.argtypes = [C.c_char_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+                                            C.c_double, _dp, _dp, _dp]
         L.remd_exchange_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_long, _ip, _dp, _dp,
                                          _dp, _dp, _dp, _ip, _ip]
         _LIB = L
@@ -487,6 +489,17 @@ def read_chk(path, nmol):
                                _p(sc)))
     return ReplicaState(r, v, q, p, m, I, sc[0], sc[1], sc[2], sc[3:6].copy(), sc[6],
                         sc[7:10].copy())
+
+
+def write_chk_arrays(path, nsite, st: ReplicaState, prop):
+    """IOManager::WriteCheckPoint from host arrays (remd_write_chk_arrays): the
+    state in the remd_read_chk convention and the 26 Property-line numbers."""
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    n = len(st.r)
+    sc = f([st.s, st.Ps, st.Q, *st.Pv, st.W, *st.L])
+    _check(lib().remd_write_chk_arrays(path.encode(), n, nsite, _p(f(st.r)), _p(f(st.v)), _p(f(st.q)),
+                                       _p(f(st.p)), float(st.m[0]), _p(f(st.I[0])), _p(sc),
+                                       _p(f(prop))))
 
 
 def exchange_host(ntemp, npress, pconstant, step, index, T, P, pot, vol, u):

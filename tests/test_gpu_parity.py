@@ -265,6 +265,38 @@ def test_device_exchange_equals_host_exchange():
         eng.execute_device()
 
 
+def test_write_chk_on_the_reference_input(tmp_path):
+    """remd_write_chk on the reference's test input (test/input/gpu0000.chk):
+    every line but the last is the reference file's bytes; the last, the
+    Property line, holds the engine's own numbers for that state, checked
+    against the FP64 oracle."""
+    from remd_b200.inputs import UNIT_PRESS, UNIT_TEMP
+    spec = golden_spec()
+    st = read_chk(f"{GOLDEN}/gpu0000.chk")
+    st.T, st.P = golden_conditions()
+    eng = E.REMDGPU([single(spec, st)], precision="fp64")
+    eng.write_chk(0, str(tmp_path / "e.chk"))
+    mine = open(tmp_path / "e.chk").read().splitlines()
+    ref = open(f"{GOLDEN}/gpu0000.chk").read().splitlines()
+    assert len(mine) == len(ref) and mine[:-1] == ref[:-1]
+    prop = np.array([float(x) for x in mine[-1].split()])
+    assert len(prop) == 26
+    orc = O.Oracle(spec, st)
+    orc.initialize_property()
+    po, avg = orc.prop(), orc.average()
+    assert prop[0] == 0.0                                       # time: no MD step yet
+    for k, key in [(1, "pot"), (2, "tra"), (3, "rot"), (4, "kin"), (9, "tot")]:
+        assert prop[k] == pytest.approx(po[key], rel=1e-6), key
+    assert abs(prop[10]) <= 1e-6 * abs(po["tot"])               # ham = tot - H0 = 0
+    assert prop[14] == pytest.approx(po["kin"] / (3 * spec.nmol) * UNIT_TEMP, rel=1e-6)
+    prs = np.array([avg[8], avg[9], avg[10], avg[7]]) * UNIT_PRESS
+    assert np.allclose(prop[15:19], prs, rtol=1e-5) and np.allclose(prop[22:26], prs, rtol=1e-5)
+    assert np.allclose(prop[19:22], po["vir"], rtol=1e-6)
+    tmo = (st.v * st.m[:, None] / (st.L * st.s)).sum(axis=0)  # Molecules::Momentum
+    assert np.allclose(prop[11:14], tmo, rtol=1e-5, atol=1e-9 * np.abs(st.v * st.m[:, None] / st.L).sum())
+    eng.close()
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_reference_regression_input(prec):
     """test/input/gpu0000.chk through the engine: interval 0 against the

@@ -105,6 +105,42 @@ def test_chk_round_trip(tmp_path):
     assert [len(l.split()) for l in new_lines] == [len(l.split()) for l in ref_lines[:len(new_lines)]]
 
 
+def _property_line(path):
+    return np.array([float(x) for x in open(path).read().splitlines()[-1].split()])
+
+
+def test_chk_writer_reproduces_the_reference_file_byte_for_byte(tmp_path):
+    """The reference's own test input (test/input/gpu0000.chk, written by its
+    IOManager::WriteCheckPoint) read and written back: every byte equal,
+    including the Property line (src/io_manager.cxx:632)."""
+    st = E.read_chk(f"{GOLDEN}/gpu0000.chk", 150)
+    prop = _property_line(f"{GOLDEN}/gpu0000.chk")
+    assert len(prop) == 26
+    E.write_chk_arrays(str(tmp_path / "x.chk"), 4, st, prop)
+    assert open(tmp_path / "x.chk", "rb").read() == open(f"{GOLDEN}/gpu0000.chk", "rb").read()
+
+
+@pytest.mark.parametrize("name", ["tip4p_tube_npz", "tip5p_bulk_nvt", "tip3p_slit_nve"])
+def test_chk_writer_equals_reference_operators(tmp_path, name):
+    """Against the reference's own operator<< for Vector and Property
+    (src/vector.h:141-147, src/variables.h:51-74) in WriteCheckPoint's statement
+    order, on a reference object after InitializeProperty and 20 MD steps."""
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    from tests.common import load_case
+    spec, st, _ = load_case(name)
+    ref = O.Reference(spec, st, spec.moltype_file, variant="slitwall" if spec.confined == 2 else "generic")
+    ref.initialize_property()
+    ref.execute_steps(20)
+    ref.write_chk(str(tmp_path / "ref.chk"))
+    g = ref.get()
+    from remd_b200.inputs import ReplicaState
+    mine = ReplicaState(g["r"], g["v"], g["q"], g["p"], st.m, st.I, g["s"], g["Ps"], g["Q"], g["Pv"],
+                        g["W"], g["L"], g["T"], g["P"])
+    E.write_chk_arrays(str(tmp_path / "mine.chk"), spec.moltype.nsite, mine, ref.property_line())
+    assert open(tmp_path / "mine.chk", "rb").read() == open(tmp_path / "ref.chk", "rb").read()
+
+
 @pytest.mark.parametrize("nt,npr,pcon", [(4, 2, 1), (8, 1, 0), (1, 6, 2), (5, 3, 3), (16, 4, 1)])
 def test_exchange_host_equals_oracle(nt, npr, pcon):
     rng = np.random.default_rng(nt * 100 + npr)
