@@ -64,12 +64,18 @@ def parse_args(argv=None):
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="config 4: skip the bounded serving sample (config 5's first --jobs jobs)")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
-    ap.add_argument("--study", choices=["drift"], default=None,
+    ap.add_argument("--study", choices=["drift", "lists"], default=None,
                     help="drift: NP Hamiltonian drift of the precision-study system (config 3), "
                          "FP32 form on every replica and FP64 vs FP32 on a subset")
     ap.add_argument("--drift-ps", type=float, default=100.0, help="drift study length (ps)")
     ap.add_argument("--drift-subset", type=int, default=8, help="replicas run in both forms")
+    ap.add_argument("--drift-ref-ps", type=float, default=0.4,
+                    help="drift study: window of the reference CPU FP64 leg (ps; 0 = skip)")
+    ap.add_argument("--drift-ref-replicas", type=int, default=4,
+                    help="drift study: replicas of the reference CPU FP64 leg")
     ap.add_argument("--equil-rounds", type=int, default=10,
                     help="untimed relaxation rounds of 20 steps + init_scaling")
     a = ap.parse_args(argv)
@@ -334,17 +340,15 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
             "intervals": stats["intervals_done"], "busy_s": stats["busy_s"]}
 
 
-def serving_arm(args, rank, world, local):
-    import torch
+def serving_sample(seed, njobs, warmup, budget_gib, dev, world):
+    """The first `njobs` jobs of the seeded config-5 stream, served (continuous
+    batching) and then one at a time, after `warmup` one-interval jobs."""
     from remd_b200 import systems as S
-    dev = local
-    njobs = args.jobs
-    jobs = make_jobs(args.seed + 1000 * rank, njobs)
-    arrivals = S.config5_arrivals(args.seed + 1000 * rank, njobs)
-    torch.cuda.set_device(dev)
-    budget = int(args.budget_gib * (1 << 30))
+    jobs = make_jobs(seed, njobs)
+    arrivals = S.config5_arrivals(seed, njobs)
+    budget = int(budget_gib * (1 << 30))
     # warm-up: the first W jobs, one interval each (library load, context, graph capture)
-    warm = [(e, 1) for e, _ in jobs[:max(args.warmup, 1)]]
+    warm = [(e, 1) for e, _ in jobs[:max(warmup, 1)]]
     run_stream(warm, np.zeros(len(warm)), budget, dev, False, seed0=77)
     clocks = ClockSampler(dev)
     barrier(world)
@@ -352,6 +356,17 @@ def serving_arm(args, rank, world, local):
     barrier(world)
     clk = clocks.stop()
     single = run_stream(jobs, arrivals, budget, dev, True)
+    return jobs, warm, batched, single, clk
+
+
+def serving_arm(args, rank, world, local):
+    import torch
+    from remd_b200 import systems as S
+    dev = local
+    njobs = args.jobs
+    torch.cuda.set_device(dev)
+    jobs, warm, batched, single, clk = serving_sample(args.seed + 1000 * rank, njobs, args.warmup,
+                                                      args.budget_gib, dev, world)
     value, max_s, total = aggregate(batched["makespan_s"] * 1e3, batched["mol_steps"], world)
     if rank == 0:
         n = [e.spec.nmol for e, _ in jobs]
@@ -447,6 +462,41 @@ def drift_study(args, rank, world, local):
         _, H = _drift_run(h, nint, dt_ps)
         out[prec] = (H, time.perf_counter() - t0)
         h.close()
+    # the reference's own FP64 CPU build (oracle/_ref, generic switched path,
+    # replica-parallel) from the first starts of the subset over a shorter
+    # window, beside the engine's FP64 and FP32 forms over the same window
+    ref_leg = None
+    if args.drift_ref_ps > 0:
+        from oracle import oracle as O
+        if O.reference_available():
+            samp = 10   # MD steps between H samples
+            dts = e0.spec.dt * 1e-3 * samp
+            nref = min(args.drift_ref_replicas, len(sub_states))
+            nint_r = max(3, int(round(args.drift_ref_ps / dts)))
+            starts = sub_states[:nref]
+            tr = (np.arange(nint_r) + 1) * dts * 1e-3
+            refs = [O.Reference(e0.spec, st, e0.spec.moltype_file) for st in starts]
+            for r in refs:
+                r.initialize_property()
+            Hr = np.zeros((nint_r, nref))
+            t0 = time.perf_counter()
+            for k in range(nint_r):
+                O.reference_parallel_steps(refs, samp, os.cpu_count() or 1)
+                Hr[k] = [r.average()[11] for r in refs]
+            wall_r = time.perf_counter() - t0
+            short = S.Ensemble("drift_ref", e0.spec, nref, 1, np.array([s_.T for s_ in starts]),
+                               np.array([s_.P for s_ in starts]), starts)
+            eng_short = {}
+            for prec in ("fp64", "fp32"):
+                h = E.REMDGPU([short], precision=prec, device=dev, interval=samp)
+                _, H = _drift_run(h, nint_r, dts)
+                eng_short[prec] = _drift_stats(tr, H, nmol)
+                h.close()
+            ref_leg = {"duration_ps": nint_r * dts, "samples": nint_r, "sample_steps": samp,
+                       "reference_cpu_fp64": dict(_drift_stats(tr, Hr, nmol), wall_s=wall_r,
+                                                  threads=os.cpu_count(),
+                                                  build="oracle/_ref generic FP64 (-DSWITCHING)"),
+                       "engine_fp64": eng_short["fp64"], "engine_fp32": eng_short["fp32"]}
     line = {"metric": "NP Hamiltonian drift", "unit": "kJ/mol per ns per molecule",
             "value": _drift_stats(t, H32, nmol)["rate_median_abs"], "higher_is_better": False,
             "study": "drift", "duration_ps": nint * dt_ps, "intervals": nint,
@@ -457,8 +507,54 @@ def drift_study(args, rank, world, local):
             "subset": [int(k) for k in sub],
             "fp32_subset": dict(_drift_stats(t, out["fp32"][0], nmol), wall_s=out["fp32"][1]),
             "fp64_subset": dict(_drift_stats(t, out["fp64"][0], nmol), wall_s=out["fp64"][1]),
+            "short_window_vs_reference_cpu": ref_leg,
             "data": "synthetic"}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ force step per system (list builds)
+def lists_study(args, rank, world, local):
+    """Force-step time (CUDA events over 50 MD steps, list rebuilds included:
+    remd_profile_steps) at fixed tile 32 and several skins, for the config-4
+    batch and for the largest systems of the serving stream (N = 4096: a 50 A
+    TIP5P bulk box, a 1.4 um TIP4P nanotube, a 115 A TIP3P slit; 8 replicas
+    each), with a hash of the positions and momenta after one more interval
+    (the trajectory does not depend on how the lists are built)."""
+    import ctypes
+    import hashlib
+
+    import torch
+    from remd_b200 import engine as E
+    from remd_b200 import systems as S
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    out = {}
+
+    def measure(name, ens, skin, nsteps):
+        eng = E.REMDGPU(ens, precision="fp32", device=local, interval=10)
+        eng.set_tuning(32, skin)
+        eng.execute_nsteps(20)
+        prof = (ctypes.c_double * 2)()
+        E._check(E.lib().remd_profile_steps(eng.h, nsteps, prof))
+        eng.ExecuteSteps(np.concatenate([e.T for e in ens]), np.concatenate([e.P for e in ens]))
+        h = hashlib.sha1()
+        for r in range(min(eng.nrep, 8)):
+            g = eng.ConvertVariablesToHost(r)
+            h.update(g["r"].tobytes())
+            h.update(g["p"].tobytes())
+        out[name] = {"force_ms": prof[1], "integrate_ms": prof[0], "skin": skin, "tile": 32,
+                     "trajectory_sha1": h.hexdigest()}
+        eng.close()
+
+    c4 = S.config4(seed=4)
+    for skin in (0.2, 0.6, 1.0):
+        measure(f"config4_skin{skin}", c4, skin, 50)
+    for model, confined, wall, rc in [("tip5p", 0, 0.0, 12.0), ("tip4p", 1, 7.0, 10.0), ("tip3p", 2, 12.0, 11.0)]:
+        e = S.make_ensemble("big", model, confined, 4096, wall, rc, rc - 1.0, 4, 2, 250, 350, 0.1e6, 0.1e6, 41)
+        for skin in (0.2, 1.0):
+            measure(f"n4096_{model}_confined{confined}_skin{skin}", [e], skin, 30)
+    print(json.dumps({"study": "lists", "unit": "ms per MD step", "systems": out}), flush=True)
 
 
 # ------------------------------------------------------------------ engine arm
@@ -605,14 +701,22 @@ def engine_arm(args, rank, world, local):
     E._check(E.lib().remd_measure_fp32_peak(dev, ctypes.byref(peak)))
     achieved = flops / (force_ms * 1e-3) / 1e12
     roof = {"bound": "fp32",
-            "kernel": "force step: k_force_lists (head, list rebuild, pairs within rcut) + "
+            "kernel": "force step: k_replica_head (PsPv + D4, list decision, cell sort) + "
+                      "k_force_lists (list rebuild, pairs within rcut) + "
                       "k_force_pairs (pair forces, wall, A2M)",
             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value,
             "peak_source": "measured: register-resident FP32 FMA chains on all SMs "
                            "(remd_measure_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
             "traffic": profile_traffic(), "pairs_per_launch": pairs,
-            "flops_per_launch": flops, "force_ms": force_ms, "integrate_ms": integ_ms}
+            "flops_per_launch": flops, "force_ms": force_ms, "integrate_ms": integ_ms,
+            "timing": "force_ms: CUDA events around the force launches of 50 MD steps run one "
+                      "launch chain at a time (remd_profile_steps, rebuilds included)"}
+    # the same FLOPs over the MD step of the timed schedule (the interval graph's
+    # concurrent chains; the step also holds the integrate and head kernels)
+    step_ms = (max_ms / args.steps) / args.interval
+    roof["in_timed_schedule"] = {"ms_per_md_step": step_ms, "achieved": flops / (step_ms * 1e-3) / 1e12,
+                                 "frac": flops / (step_ms * 1e-3) / 1e12 / peak.value}
 
     acc = None if args.no_accuracy else force_accuracy(eng, ens, dev)
 
@@ -673,6 +777,22 @@ def engine_arm(args, rank, world, local):
                  "sample": f"one replica of each of the {len(ens)} ensembles, alone, "
                            f"{psteps} steps each (one launch sequence per replica)"}
 
+    # a bounded sample of the serving stream (config 5), beside the batch
+    serving = None
+    if not args.no_serving and args.config == 4 and rank == 0 and world == 1:
+        jobs, _, sb, s1, _ = serving_sample(5, args.jobs, 1, args.budget_gib, dev, 1)
+        serving = {"workload": f"config 5: the first {len(jobs)} jobs of the seeded Poisson stream "
+                               f"(nmol {min(e.spec.nmol for e, _ in jobs)}-"
+                               f"{max(e.spec.nmol for e, _ in jobs)}, "
+                               f"{sum(e.nreplica for e, _ in jobs)} replicas)",
+                   "served_mol_steps_per_s": sb["value"], "one_at_a_time_mol_steps_per_s": s1["value"],
+                   "speedup_vs_one_at_a_time": sb["value"] / s1["value"],
+                   "p50_interval_ms": sb["p50_interval_ms"], "p99_interval_ms": sb["p99_interval_ms"],
+                   "p50_job_s": sb["p50_job_s"], "p99_job_s": sb["p99_job_s"],
+                   "intervals": sb["intervals"], "jobs_done": sb["jobs_done"],
+                   "interval_latency": "wall time of one server round: admission, any batch change, "
+                                       "the interval's graph launch and the averages' read-back"}
+
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         nst = args.cpu_steps or 2
@@ -691,6 +811,7 @@ def engine_arm(args, rank, world, local):
                             "p99_interval_ms": float(np.percentile(ms, 99)),
                             "samples": len(ms)},
                 "accuracy": acc,
+                "serving": serving,
                 "plain_fp64": plain,
                 "speedup_vs_plain_fp64": (value / world / plain["value"]) if plain else None,
                 "wall_s": wall, "interval_ms": [round(x, 3) for x in ms],
@@ -707,6 +828,8 @@ def main():
             reference_arm(args, rank, world)
         elif args.study == "drift":
             drift_study(args, rank, world, local)
+        elif args.study == "lists":
+            lists_study(args, rank, world, local)
         elif args.config == 5:
             serving_arm(args, rank, world, local)
         else:

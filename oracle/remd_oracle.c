@@ -5,7 +5,7 @@
  * Every function follows the reference file:line named in its comment, with
  * the same floating-point operation order, so that a build with the same
  * compiler flags as oracle/_ref agrees with the reference to rounding.
- * Deliberate departures (each listed in DESIGN.md's quirk table):
+ * Deliberate departures from the reference CPU code:
  *   - the cylinder table lookup clamps its base index to nfwall-2 instead of
  *     reading one entry past the table (src/force_calculator.cxx:1549-1551);
  *   - confined=2 (slit) follows the reference GPU kernel: wall force

@@ -49,6 +49,7 @@ struct remd_engine_s {
   std::vector<int> order2;         // the same per chain: chain k's tiles [chain_tile[k], chain_tile[k+1])
   int nchain = 1;                  // independent chains of the interval graph
   int chain_tile[kMaxChains + 1] = {};
+  int chain_rep[kMaxChains + 1] = {};   // chain k's replicas [chain_rep[k], chain_rep[k+1])
   int* d_order2 = nullptr;
   std::vector<double> curT, curP;
   std::vector<double> wall_h;
@@ -72,6 +73,11 @@ struct remd_engine_s {
   unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
   long long last_pairs = 0;
   long long steps_done = 0;        // MD steps run (the simulated time of the .chk Property line)
+  cudaMemPool_t mempool = nullptr;  // the pool comes from this memory pool (serving loop), else cudaMalloc
+  int pinned_cap = 0;               // replicas the pinned host buffers hold
+  int2* d_carry_src = nullptr;      // per replica: {old first molecule, old replica} of a carried replica
+  int* d_carry_ens = nullptr;       // per ensemble: old ensemble or -1
+  int* d_ens_nrep = nullptr;        // per ensemble: replicas
   size_t bytes = 0;
   // (volume, potential) histograms per condition slot, per ensemble (own allocations)
   std::vector<HistEns> hist;        // host copy of d_hist (device pointers inside)
@@ -190,8 +196,12 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       cut.push_back(best);
     }
     h->nchain = K;
-    for (int k = 0; k < K; k++) h->chain_tile[k] = h->rc[cut[k]].tile_off;
+    for (int k = 0; k < K; k++) {
+      h->chain_tile[k] = h->rc[cut[k]].tile_off;
+      h->chain_rep[k] = cut[k];
+    }
     h->chain_tile[K] = (int)h->tiles.size();
+    h->chain_rep[K] = h->nrep;
     h->order2.clear();
     for (int k = 0; k < K; k++)
       for (int t : h->order)
@@ -223,7 +233,12 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
       nt * 4,                          // 31 order
       (h->prec == kF32) ? N * 4 : 0,   // 32 nt_cnt (FP32 per-step list counts)
       N * sizeof(int4),                // 33 com (FP32 current fixed-point centres)
-      nt * 4,                          // 34 order per half (two-chain interval graph)
+      nt * 4,                          // 34 order per chain (multi-chain interval graph)
+      nr * sizeof(CellGrid),           // 35 cell grid + rebuild decision per replica
+      nr * (size_t)(kMaxCells + 1) * 4,   // 36 cell offsets per replica
+      N * sizeof(int4),                // 37 centres sorted by cell
+      nr * sizeof(int2),               // 38 carried replicas' sources (serving batch changes)
+      (size_t)h->nens * 4, (size_t)h->nens * 4,   // 39 carried ensembles' sources, 40 replicas per ensemble
   };
   offs.clear();
   total = 0;
@@ -233,12 +248,19 @@ static void layout(remd_engine_s* h, std::vector<size_t>& offs, size_t& total) {
   }
 }
 
+static void free_pool(remd_engine_s* h) {
+  if (h->mempool) cudaFreeAsync(h->pool, h->stream);
+  else cudaFree(h->pool);
+  h->pool = nullptr;
+}
+
 static remd_status allocate(remd_engine_s* h) {
   std::vector<size_t> offs;
   size_t total;
   layout(h, offs, total);
-  if (h->pool) { cudaFree(h->pool); h->pool = nullptr; }
-  cudaError_t e = cudaMalloc(&h->pool, total);
+  if (h->pool) { free_pool(h); }
+  cudaError_t e = h->mempool ? cudaMallocFromPoolAsync(&h->pool, total, h->mempool, h->stream)
+                             : cudaMalloc(&h->pool, total);
   if (e != cudaSuccess) {
     set_error(std::string("device allocation of ") + std::to_string(total) + " bytes: " + cudaGetErrorString(e));
     return REMD_ERR_OOM;
@@ -289,6 +311,19 @@ static remd_status allocate(remd_engine_s* h) {
   d.com = reinterpret_cast<int4*>(b + offs[33]);
   d.tile0 = 0;
   h->d_order2 = reinterpret_cast<int*>(b + offs[34]);
+  d.cgrid = reinterpret_cast<CellGrid*>(b + offs[35]);
+  d.cell_start = reinterpret_cast<int*>(b + offs[36]);
+  d.cell_com = reinterpret_cast<int4*>(b + offs[37]);
+  h->d_carry_src = reinterpret_cast<int2*>(b + offs[38]);
+  h->d_carry_ens = reinterpret_cast<int*>(b + offs[39]);
+  h->d_ens_nrep = reinterpret_cast<int*>(b + offs[40]);
+  d.rep0 = 0;
+  d.nrep_l = h->nrep;
+  {
+    int nmax = 1;
+    for (const RepConst& c : h->rc) nmax = std::max(nmax, c.nmol);
+    d.bm_win = bitmap_window(nmax);
+  }
   h->u_cap = std::max(h->nrep / 2, 1);
   h->bytes = total;
   CK(cudaMemcpyAsync((void*)d.rc, h->rc.data(), h->rc.size() * sizeof(RepConst), cudaMemcpyHostToDevice, h->stream));
@@ -365,7 +400,6 @@ static void launch_step_integrate(remd_engine_s* h, int s) {
 }
 
 static remd_status build_graph(remd_engine_s* h) {
-  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   launch_replica_start(h->d, h->X, h->stream);
@@ -380,6 +414,8 @@ static remd_status build_graph(remd_engine_s* h) {
       dg[k].ntiles = h->chain_tile[k + 1] - h->chain_tile[k];
       dg[k].order = h->d_order2 + h->chain_tile[k];
       dg[k].tile0 = h->chain_tile[k];
+      dg[k].rep0 = h->chain_rep[k];
+      dg[k].nrep_l = h->chain_rep[k + 1] - h->chain_rep[k];
     }
     cudaEventRecord(h->ev_fork, h->stream);
     for (int k = 1; k < h->nchain; k++) cudaStreamWaitEvent(h->stream2[k - 1], h->ev_fork, 0);
@@ -413,6 +449,22 @@ static remd_status build_graph(remd_engine_s* h) {
     set_error(std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ce));
     return REMD_ERR_CUDA;
   }
+  // an existing executable graph of the same topology (the handle's previous
+  // graph, or the one a carried handle took over) is updated in place, which
+  // costs far less than instantiating a new one
+  if (h->gexec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(h->gexec, g, &info) == cudaSuccess) {
+      cudaGraphDestroy(g);
+      h->graph_tile = h->tile;
+      h->graph_exchange = h->exch_enabled;
+      h->graph_hist = h->hist_on;
+      return REMD_OK;
+    }
+    cudaGetLastError();
+    cudaGraphExecDestroy(h->gexec);
+    h->gexec = nullptr;
+  }
   cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) {
@@ -437,29 +489,6 @@ static long long host_pairs(remd_engine_s* h) {
 
 namespace remd {
 
-// ---- internals used by the serving loop (server.cu) ----
-remd_status engine_set_h0(remd_handle h, const double* H0) {
-  std::vector<RepState> st(h->nrep);
-  CK(cudaStreamSynchronize(h->stream));
-  CK(cudaMemcpy(st.data(), h->X, st.size() * sizeof(RepState), cudaMemcpyDeviceToHost));
-  for (int k = 0; k < h->nrep; k++) st[k].H0 = H0[k];
-  CK(cudaMemcpy(h->X, st.data(), st.size() * sizeof(RepState), cudaMemcpyHostToDevice));
-  return REMD_OK;
-}
-
-// Per-ensemble exchange set-up: grids (2 per ensemble), Philox seeds, next step,
-// and the condition-slot -> replica index (per replica, ensemble-local).
-remd_status engine_set_exchange(remd_handle h, const int* grids, const unsigned long long* seeds,
-                                const long long* steps, const int* index) {
-  CK(cudaMemcpyAsync(h->d_grid, grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_seed, seeds, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_step, steps, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_index, index, h->nrep * 4, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  h->exch_enabled = true;
-  return REMD_OK;
-}
-
 remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaMemcpy(steps, h->d_step, h->nens * 8, cudaMemcpyDeviceToHost));
@@ -467,23 +496,103 @@ remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
   return REMD_OK;
 }
 
-// Conditions to apply (with the exchange tail) at the start of the next interval.
-remd_status engine_set_pending_conditions(remd_handle h, const double* T, const double* P) {
-  CK(cudaStreamSynchronize(h->stream));
-  CK(cudaMemcpy(h->dT, T, h->nrep * 8, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(h->dP, P, h->nrep * 8, cudaMemcpyHostToDevice));
-  return REMD_OK;
-}
-
 size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
+
+remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
+                                const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
+                                const int* src_ens, const int* grids, const unsigned long long* seeds,
+                                const long long* steps, remd_precision prec, int device, cudaMemPool_t mempool,
+                                remd_handle* out);
 
 }  // namespace remd
 
-extern "C" {
+// A new handle that continues replicas of an existing one (the serving loop's
+// batch changes): their molecule state, scalars, pending condition and, per
+// ensemble, the exchange's index, counter and seed are copied on the device
+// from `from`, which must be on the same device with the same precision; the
+// new handle takes over its streams, pinned buffers and interval graph (updated
+// in place at the first interval when its topology allows).  `reps` entries of
+// carried replicas are not read.
+struct Carry {
+  remd_engine_s* from;
+  const int* src_rep;                // per new replica: its replica in `from`, or -1
+  const int* src_ens;                // per new ensemble: its ensemble in `from`, or -1
+  const int* grids;                  // ntemp, npress per ensemble (device exchange)
+  const unsigned long long* seeds;   // per ensemble (read for new ensembles)
+  const long long* steps;            // per ensemble (read for new ensembles)
+  cudaMemPool_t mempool;             // the new pool's memory pool (may be NULL)
+};
 
-remd_status remd_create(const remd_system_desc* systems, int nens, const int* reps_per_ens,
-                        const remd_replica_init* reps, remd_precision prec, int device,
-                        remd_handle* out) {
+// The device exchange configuration of a carried handle and the carried
+// replicas' state, then the initial force of every replica (forces are a pure
+// function of the positions, so a carried replica's are the ones it had), H0 of
+// the new replicas (InitializeProperty) and the carried replicas' scalars again
+// (their H0 and gkT, which the property pass recomputes).
+static remd_status carry_in(remd_engine_s* h, const Carry* cy) {
+  remd_engine_s* o = cy->from;
+  std::vector<int2> src(h->nrep);
+  for (int k = 0; k < h->nrep; k++) {
+    const int so = o ? cy->src_rep[k] : -1;
+    src[k] = make_int2(so >= 0 ? o->rc[so].mol_off : -1, so);
+  }
+  std::vector<int> sens(cy->src_ens, cy->src_ens + h->nens);
+  if (!o) std::fill(sens.begin(), sens.end(), -1);
+  std::vector<int> idx(h->nrep);
+  for (int e = 0; e < h->nens; e++)
+    for (int k = 0; k < h->ens_nrep[e]; k++) idx[h->ens_rep_off[e] + k] = k;
+  CK(cudaMemcpyAsync(h->d_carry_src, src.data(), src.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_carry_ens, sens.data(), sens.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_ens_nrep, h->ens_nrep.data(), h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_grid, cy->grids, 2 * h->nens * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_seed, cy->seeds, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_step, cy->steps, h->nens * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_index, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  auto carry = [&](bool molecules) {
+    if (!o) return;
+    launch_carry(h->d, o->d, h->tile, h->d_carry_src, h->X, o->X, h->dT, h->dP, o->dT, o->dP, h->nens,
+                 h->d_carry_ens, h->d_rep_off, o->d_rep_off, h->d_ens_nrep, h->d_index, o->d_index, h->d_step,
+                 o->d_step, h->d_seed, o->d_seed, molecules, h->stream);
+  };
+  carry(true);
+  launch_pack(h->d, h->prec, h->tile, h->stream);
+  launch_force(h->d, h->X, h->X, h->prec, true, h->tile, h->stream);
+  launch_replica_props(h->d, h->X, h->stream);
+  carry(false);
+  CK(cudaGetLastError());
+  h->exch_enabled = true;
+  // the host copies of the current conditions (read by remd_execute_steps)
+  if (o)
+    for (int k = 0; k < h->nrep; k++)
+      if (cy->src_rep[k] >= 0) { h->curT[k] = o->curT[cy->src_rep[k]]; h->curP[k] = o->curP[cy->src_rep[k]]; }
+  return sync_and_check(h);
+}
+
+// A carried handle that could not be built gives the previous handle back what
+// it took over (streams, events, graph, pinned buffers), then is destroyed: the
+// previous batch stays usable.
+static void undo_carry(remd_engine_s* h, const Carry* cy) {
+  if (cy && cy->from) {
+    remd_engine_s* o = cy->from;
+    if (h->stream) cudaStreamSynchronize(h->stream);   // nothing of h's is in flight any more
+    if (h->pool) free_pool(h);
+    if (!o->stream) { o->stream = h->stream; h->stream = nullptr; }
+    if (!o->ev_fork) { o->ev_fork = h->ev_fork; h->ev_fork = nullptr; }
+    for (int k = 0; k < kMaxChains - 1; k++) {
+      if (!o->stream2[k]) { o->stream2[k] = h->stream2[k]; h->stream2[k] = nullptr; }
+      if (!o->ev_join[k]) { o->ev_join[k] = h->ev_join[k]; h->ev_join[k] = nullptr; }
+    }
+    if (!o->gexec) { o->gexec = h->gexec; h->gexec = nullptr; }
+    if (!o->hT) {
+      o->hT = h->hT; o->hP = h->hP; o->havg = h->havg; o->pinned_cap = h->pinned_cap;
+      h->hT = h->hP = h->havg = nullptr;
+    }
+  }
+  remd_destroy(h);
+}
+
+static remd_status create_impl(const remd_system_desc* systems, int nens, const int* reps_per_ens,
+                               const remd_replica_init* reps, remd_precision prec, int device,
+                               const Carry* cy, remd_handle* out) {
   if (!systems || nens < 1 || !reps_per_ens || !reps || !out) {
     set_error("remd_create: null argument");
     return REMD_ERR_INVALID;
@@ -533,7 +642,26 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
     int c0 = 0;
     valid_model(s, &c0);
     for (int k = 0; k < reps_per_ens[e]; k++, rep++) {
-      const remd_replica_init& ri = reps[rep];
+      const int src = (cy && cy->from) ? cy->src_rep[rep] : -1;
+      remd_replica_init ri = reps[rep];
+      std::vector<double> cm, ci;   // a carried replica's mass and inertia columns
+      if (src >= 0) {
+        const RepConst& o = cy->from->rc[src];
+        cm.assign(s.nmol, o.mass);
+        ci.resize(3 * (size_t)s.nmol);
+        for (int i = 0; i < s.nmol; i++)
+          for (int x = 0; x < 3; x++) ci[3 * i + x] = o.I[x];
+        ri.r = ri.v = ri.q = ri.p = cm.data();   // not read: the state is copied on the device
+        ri.mass = cm.data();
+        ri.inertia = ci.data();
+        ri.Q = o.Q;
+        ri.W = o.W;
+        ri.T = cy->from->curT[src];
+        ri.P = cy->from->curP[src];
+        ri.s = 1.0;
+        ri.Ps = 0.0;
+        for (int x = 0; x < 3; x++) { ri.Pv[x] = 0.0; ri.L[x] = 1.0; }   // replaced on the device
+      }
       if (!ri.r || !ri.v || !ri.q || !ri.p || !ri.mass || !ri.inertia) {
         set_error("replica " + std::to_string(rep) + ": null state array");
         delete h;
@@ -621,26 +749,56 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
   }
   h->nrep = rep;
   h->N = mol;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      force_kernel_setup() != cudaSuccess) {
-    set_error("cannot set up device/stream");
-    delete h;
-    return REMD_ERR_CUDA;
-  }
-  for (int k = 0; k < kMaxChains - 1; k++)
-    if (cudaStreamCreateWithFlags(&h->stream2[k], cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess) {
-      set_error("cannot create the interval graph's streams");
-      remd_destroy(h);
+  h->mempool = cy ? cy->mempool : nullptr;
+  if (cy && cy->from) {
+    remd_engine_s* o = cy->from;
+    h->stream = o->stream;
+    h->ev_fork = o->ev_fork;
+    o->stream = nullptr;
+    o->ev_fork = nullptr;
+    for (int k = 0; k < kMaxChains - 1; k++) {
+      h->stream2[k] = o->stream2[k];
+      h->ev_join[k] = o->ev_join[k];
+      o->stream2[k] = nullptr;
+      o->ev_join[k] = nullptr;
+    }
+    h->gexec = o->gexec;   // re-captured and updated in place at the first interval
+    o->gexec = nullptr;
+    h->graph_tile = -1;
+    if (o->pinned_cap >= h->nrep) {
+      h->hT = o->hT; h->hP = o->hP; h->havg = o->havg;
+      h->pinned_cap = o->pinned_cap;
+      o->hT = o->hP = o->havg = nullptr;
+      o->pinned_cap = 0;
+    }
+    if (cudaSetDevice(device) != cudaSuccess || force_kernel_setup() != cudaSuccess) {
+      set_error("cannot set up device");
+      undo_carry(h, cy);
       return REMD_ERR_CUDA;
     }
+  } else {
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        force_kernel_setup() != cudaSuccess) {
+      set_error("cannot set up device/stream");
+      delete h;
+      return REMD_ERR_CUDA;
+    }
+    for (int k = 0; k < kMaxChains - 1; k++)
+      if (cudaStreamCreateWithFlags(&h->stream2[k], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess) {
+        set_error("cannot create the interval graph's streams");
+        undo_carry(h, cy);
+        return REMD_ERR_CUDA;
+      }
+  }
   remd_status st = allocate(h);
-  if (st != REMD_OK) { remd_destroy(h); return st; }
+  if (st != REMD_OK) { undo_carry(h, cy); return st; }
   // host SoA staging
   const int N = h->N;
   std::vector<double> r((size_t)N * 3), v((size_t)N * 3), q((size_t)N * 4), p((size_t)N * 4);
   for (int k = 0; k < h->nrep; k++) {
+    if (cy && cy->from && cy->src_rep[k] >= 0) continue;   // copied on the device below
     const remd_replica_init& ri = reps[k];
     const RepConst& c = h->rc[k];
     for (int i = 0; i < c.nmol; i++) {
@@ -649,13 +807,16 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
       for (int x = 0; x < 4; x++) { q[(size_t)x * N + g] = ri.q[4 * i + x]; p[(size_t)x * N + g] = ri.p[4 * i + x]; }
     }
   }
-  if ((st = upload_state(h, r, v, q, p, st0)) != REMD_OK) { remd_destroy(h); return st; }
-  if (cudaStreamSynchronize(h->stream) != cudaSuccess) { set_error("state upload failed"); remd_destroy(h); return REMD_ERR_CUDA; }
-  if (cudaMallocHost(&h->hT, h->nrep * 8) != cudaSuccess || cudaMallocHost(&h->hP, h->nrep * 8) != cudaSuccess ||
-      cudaMallocHost(&h->havg, (size_t)h->nrep * kNumAvg * 8) != cudaSuccess) {
-    set_error("pinned host allocation failed");
-    remd_destroy(h);
-    return REMD_ERR_OOM;
+  if ((st = upload_state(h, r, v, q, p, st0)) != REMD_OK) { undo_carry(h, cy); return st; }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) { set_error("state upload failed"); undo_carry(h, cy); return REMD_ERR_CUDA; }
+  if (!h->hT) {
+    if (cudaMallocHost(&h->hT, h->nrep * 8) != cudaSuccess || cudaMallocHost(&h->hP, h->nrep * 8) != cudaSuccess ||
+        cudaMallocHost(&h->havg, (size_t)h->nrep * kNumAvg * 8) != cudaSuccess) {
+      set_error("pinned host allocation failed");
+      undo_carry(h, cy);
+      return REMD_ERR_OOM;
+    }
+    h->pinned_cap = h->nrep;
   }
   // device-side exchange bookkeeping: identity index, current conditions
   {
@@ -669,20 +830,30 @@ remd_status remd_create(const remd_system_desc* systems, int nens, const int* re
         cudaMemcpy(h->dP, h->curP.data(), h->nrep * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(h->d_rep_off, roff.data(), roff.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
       set_error("upload of the condition arrays failed");
-      remd_destroy(h);
+      undo_carry(h, cy);
       return REMD_ERR_CUDA;
     }
   }
-  if ((st = initial_force(h)) != REMD_OK) { remd_destroy(h); return st; }
+  if (cy) st = carry_in(h, cy);
+  else st = initial_force(h);
+  if (st != REMD_OK) { undo_carry(h, cy); return st; }
   h->last_pairs = host_pairs(h);
   *out = h;
   return REMD_OK;
 }
 
+extern "C" {
+
+remd_status remd_create(const remd_system_desc* systems, int nens, const int* reps_per_ens,
+                        const remd_replica_init* reps, remd_precision prec, int device,
+                        remd_handle* out) {
+  return create_impl(systems, nens, reps_per_ens, reps, prec, device, nullptr, out);
+}
+
 remd_status remd_destroy(remd_handle h) {
   if (!h) return REMD_OK;
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
-  if (h->pool) cudaFree(h->pool);
+  if (h->pool) free_pool(h);
   if (h->hT) cudaFreeHost(h->hT);
   if (h->hP) cudaFreeHost(h->hP);
   if (h->havg) cudaFreeHost(h->havg);
@@ -939,13 +1110,13 @@ long long remd_last_pair_count(remd_handle h) {
   return h->last_pairs;
 }
 int remd_launches_per_interval(remd_handle h) {
-  // replica_start + per MD step (integrate, force: lists + pairs in FP32, one launch in FP64;
+  // replica_start + per MD step (integrate, replica head, force: lists + pairs in FP32, one launch in FP64;
   // with velocity scaling also the rescale and, after the first step, the closing kick)
   // + replica_end + the device exchange when enabled (and the histogram before it)
   if (!h) return 0;
   // (the multi-chain graph, without velocity scaling, launches each step kernel once per chain)
   const int chains = h->vscale ? 1 : h->nchain;
-  const int per_step = ((h->prec == kF32 ? 3 : 2) + (h->vscale ? 1 : 0)) * chains;
+  const int per_step = ((h->prec == kF32 ? 4 : 3) + (h->vscale ? 1 : 0)) * chains;
   return per_step * h->interval + (h->vscale ? h->interval - 1 : 0) + 2 + (h->exch_enabled ? 1 : 0) +
          (h->exch_enabled && h->hist_on ? 1 : 0);
 }
@@ -1434,3 +1605,22 @@ remd_status remd_histogram_read(remd_handle h, int ens, const char* dir) {
 }
 
 }  // extern "C"
+
+namespace remd {
+remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
+                                const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
+                                const int* src_ens, const int* grids, const unsigned long long* seeds,
+                                const long long* steps, remd_precision prec, int device, cudaMemPool_t mempool,
+                                remd_handle* out) {
+  if (!src_rep || !src_ens || !grids || !seeds || !steps) {
+    set_error("engine_create_carry: null argument");
+    return REMD_ERR_INVALID;
+  }
+  if (from && ((from->prec == kF64) != (prec == REMD_PREC_FP64) || from->device != device)) {
+    set_error("engine_create_carry: the previous handle has another precision or device");
+    return REMD_ERR_INVALID;
+  }
+  Carry cy{from, src_rep, src_ens, grids, seeds, steps, mempool};
+  return create_impl(systems, nens, reps_per_ens, reps, prec, device, &cy, out);
+}
+}  // namespace remd

@@ -80,6 +80,16 @@ struct Tile {
   int rep, start, count, pad;   // replica, first local molecule, molecules in tile
 };
 
+// Cell lists of a replica (rebuilt with its neighbour lists): the periodic box
+// cut into nx x ny x nz cells at least as wide as the list radius (a dimension
+// with fewer than three such cells is not cut), molecules counting-sorted by
+// cell.  cell_start holds kMaxCells + 1 offsets per replica.
+constexpr int kMaxCells = 2048;
+struct CellGrid {
+  int nx, ny, nz;
+  int rebuild;                  // the head's decision for this force step
+};
+
 // Everything a kernel needs, passed by value.
 struct DevPtrs {
   int N;                         // total molecules
@@ -102,10 +112,15 @@ struct DevPtrs {
   double* avg;                   // nrep * kNumAvg
   int* status;                   // per replica health word
   int* err;                      // global error word (bit flags)
+  CellGrid* cgrid;               // per replica: grid and rebuild decision of this force step
+  int* cell_start;               // per replica, kMaxCells + 1 offsets into cell_mol
+  int4* cell_com;                // per molecule (global index space): centres sorted by cell, .w = local index
   const double* newT;            // conditions for the next interval (per replica)
   const double* newP;
   const int* changed;            // 1 = apply the exchange tail at the interval start
   int tile0;                     // first tile of a launch over a tile range (order == NULL)
+  int rep0, nrep_l;              // replicas [rep0, rep0 + nrep_l) of a launch (per-replica kernels)
+  int bm_win;                    // words per row of the list-rebuild bitmap (kernels.cu)
 };
 
 enum : int { kErrNbrOverflow = 1, kErrNonFinite = 2, kErrHistRange = 4 };

@@ -4,12 +4,17 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "integrator.cuh"
 #include "kernels.cuh"
 
 namespace remd {
+
+constexpr int kRepThreads = 256;   // threads of the per-replica kernels
+constexpr int kBitmapMaxWords = 64; // list-rebuild bitmap window: 2048 molecules per pass
+constexpr int kCellMinPrune = 4;    // cut a replica into cells when they prune at least 4x
 
 int pack_stride(int nsite, int prec) {
   if (prec == kF32) return ((3 + 3 * nsite) + 3) / 4 * 4;   // words, 16-B multiple
@@ -125,6 +130,8 @@ __device__ inline void write_pack(const DevPtrs& d, const RepConst& c, int prec,
       body_to_space(q, c.body[k], o);
       for (int x = 0; x < 3; x++) w[3 + 3 * k + x] = o[x];
     }
+    // fixed-point centre: the cell of the molecule at the next list build
+    d.com[c.mol_off + li] = make_int4(fix_coord(r[0]), fix_coord(r[1]), fix_coord(r[2]), 0);
   }
 }
 
@@ -246,14 +253,164 @@ __global__ void __launch_bounds__(128, 7) k_integrate(DevPtrs d, const RepState*
 }
 
 // ------------------------------------------------------------------ force
-struct ForceHead {
-  double L[3];
-  int rebuild;
-};
+// Cell of a fixed-point box fraction x = (r - 1/2) 2^32 on an n-cell axis:
+// floor(r n), exact (r 2^32 = x + 2^31 as an unsigned word).
+__device__ __forceinline__ int cell_coord(int x, int n) {
+  const unsigned u = (unsigned)x + 0x80000000u;
+  return (int)(((unsigned long long)u * (unsigned)n) >> 32);
+}
 
-// Neighbour-list rebuild for the molecules of this tile: every molecule of the
-// replica is tested against (rcut+skin), 128 candidates at a time from shared
-// memory (all lanes read the same candidate: a broadcast).
+// Radius the list build tests (FP32 form): rcut + skin widened by the
+// truncation error of its FP32 test, sqrt(3) L_max 2^-16, and a relative 1e-5.
+// The FP64 form's test radius, rcut + skin, is below it.
+__device__ inline double list_test_radius(const RepConst& c, const double* L) {
+  const double lmax = fmax(fmax(L[0], L[1]), L[2]);
+  return (c.rc + c.skin + 1.7320508075688772 * lmax * (1.0 / 65536.0)) * (1.0 + 1e-5);
+}
+
+// Cells per dimension: as many as fit at least the test radius wide, so that
+// every pair the list build keeps lies in neighbouring cells; a dimension with
+// fewer than three such cells is not cut (one cell), and the grid is coarsened
+// along its longest axis until it has at most kMaxCells cells.
+__device__ inline CellGrid cell_grid(const RepConst& c, const double* L) {
+  // a cell is wider than any component the FP32 test can keep (its truncated
+  // differences err by less than L 2^-16 per component), so the lists equal
+  // those of a test against every molecule of the replica
+  const double lmax = fmax(fmax(L[0], L[1]), L[2]);
+  const double rw = list_test_radius(c, L) + 2.0 * lmax * (1.0 / 65536.0);
+  int n[3];
+  for (int x = 0; x < 3; x++) {
+    const double q = L[x] / rw;
+    n[x] = (q >= 3.0) ? (int)fmin(floor(q), (double)kMaxCells) : 1;   // NaN -> 1
+  }
+  while ((long long)n[0] * n[1] * n[2] > kMaxCells) {
+    const int m = (n[0] >= n[1] && n[0] >= n[2]) ? 0 : (n[1] >= n[2] ? 1 : 2);
+    n[m] = (n[m] - 1 >= 3) ? n[m] - 1 : 1;
+  }
+  // a candidate from the cells costs several times one of the all-molecule scan
+  // (gathered, per lane, versus a shared-memory broadcast): cut the box only
+  // where the neighbouring cells hold at most 1/kCellMinPrune of the replica
+  const int stencil = (n[0] > 1 ? 3 : 1) * (n[1] > 1 ? 3 : 1) * (n[2] > 1 ? 3 : 1);
+  if ((long long)stencil * kCellMinPrune > (long long)n[0] * n[1] * n[2]) n[0] = n[1] = n[2] = 1;
+  CellGrid g;
+  g.nx = n[0]; g.ny = n[1]; g.nz = n[2];
+  g.rebuild = 1;
+  return g;
+}
+
+__device__ inline int cell_of(const int4 x, const CellGrid& g) {
+  return (cell_coord(x.z, g.nz) * g.ny + cell_coord(x.y, g.ny)) * g.nx + cell_coord(x.x, g.nx);
+}
+
+// Per-replica head of a force step, one block per replica of the launch:
+//  * warp 0 sums the integrate kernel's partials (lane-strided, then a
+//    butterfly, so the order depends only on the replica's record count) and
+//    lane 0 runs PsPv and D4 (src/integrator.cxx:132-172, 604-632), writes the
+//    replica's scalars to Xout and decides whether its neighbour lists must be
+//    rebuilt: pairs now within rc were within rc + skin at the build if
+//    2 max|displacement| + rc (max_d Lbuild_d / L_d - 1) <= skin;
+//  * when they must, the block counting-sorts the replica's molecules by cell
+//    (cell_grid) into cell_start / cell_com; k_force_lists then tests each
+//    molecule against the molecules of its 27 (tube: 3, slit: 9) neighbouring
+//    cells only.  The order inside a cell is arbitrary: the lists are emitted
+//    in ascending j from a bitmap (build_lists), so they do not depend on it.
+// This replaces the reference's per-replica z-sort of the molecules
+// (sort, src/sort.cu:373-459; quicksort_key, src/quicksort.cu:214-276).
+template <bool FORCE_ONLY>
+__global__ void __launch_bounds__(kRepThreads) k_replica_head(DevPtrs d, const RepState* __restrict__ Yin,
+                                                              RepState* __restrict__ Xout) {
+  __shared__ int cnt[kMaxCells];
+  __shared__ int wsum[kRepThreads / 32];
+  __shared__ CellGrid grid;
+  const int rep = d.rep0 + blockIdx.x;
+  const RepConst& c = d.rc[rep];
+  if (threadIdx.x < 32) {
+    double v[4] = {0, 0, 0, 0}, disp = 0.0;
+    if (!FORCE_ONLY) {
+      for (int k = c.warp_off + threadIdx.x; k < c.warp_off + c.nwarp; k += 32) {
+        const Part1 p = d.part1[k];
+        v[0] += p.sum_Pv[0]; v[1] += p.sum_Pv[1]; v[2] += p.sum_Pv[2];
+        v[3] += p.sum_Ps;
+        disp = fmax(disp, p.disp);
+      }
+      warp_sum<4>(v);
+      disp = warp_max(disp);
+    }
+    if (threadIdx.x == 0) {
+      RepState st = Yin[rep];
+      int rb = 1;
+      if (!FORCE_ONLY) {
+        double sPv[3] = {v[0], v[1], v[2]};
+        pspv(c, st, sPv, v[3]);
+        d4(c, st);
+        const int tix = c.tile_off;   // every tile of a replica holds the same build box
+        const double lb0 = d.Lbuild[3 * tix], lb1 = d.Lbuild[3 * tix + 1], lb2 = d.Lbuild[3 * tix + 2];
+        rb = !(lb0 == lb0);
+        if (!rb) {
+          const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
+          rb = (2.0 * disp + c.rc * (lam - 1.0) > c.skin);
+        }
+      }
+      Xout[rep] = st;   // FORCE_ONLY launches pass Xout == Yin: unchanged there
+      CellGrid g = cell_grid(c, st.L);
+      g.rebuild = rb;
+      grid = g;
+      d.cgrid[rep] = g;
+    }
+  }
+  __syncthreads();
+  if (!grid.rebuild) return;
+  const CellGrid g = grid;
+  const int ncell = g.nx * g.ny * g.nz;
+  if (ncell == 1) return;   // not cut: the list build scans every molecule
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int k = tid; k < ncell; k += T) cnt[k] = 0;
+  __syncthreads();
+  const int4* com = d.com + c.mol_off;
+  for (int li = tid; li < c.nmol; li += T) atomicAdd(&cnt[cell_of(com[li], g)], 1);
+  __syncthreads();
+  // exclusive scan of the counts: a contiguous run of cells per thread
+  const int per = (ncell + T - 1) / T;
+  const int k0 = min(tid * per, ncell), k1 = min(k0 + per, ncell);
+  int run = 0;
+  for (int k = k0; k < k1; k++) run += cnt[k];
+  int incl = run;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if ((tid & 31) >= o) incl += y;
+  }
+  if ((tid & 31) == 31) wsum[tid >> 5] = incl;
+  __syncthreads();
+  int base = incl - run;
+  for (int w = 0; w < (tid >> 5); w++) base += wsum[w];
+  int* cs = d.cell_start + (long long)rep * (kMaxCells + 1);
+  for (int k = k0; k < k1; k++) {
+    const int n = cnt[k];
+    cnt[k] = base;
+    cs[k] = base;
+    base += n;
+  }
+  if (tid == 0) cs[ncell] = c.nmol;
+  __syncthreads();
+  int4* cm = d.cell_com + c.mol_off;
+  for (int li = tid; li < c.nmol; li += T) {
+    int4 x = com[li];
+    const int pos = atomicAdd(&cnt[cell_of(x, g)], 1);
+    x.w = li;
+    cm[pos] = x;
+  }
+}
+
+// Neighbour-list rebuild for the molecules of this tile.  The list of molecule
+// i holds, in ascending j, every j that passes the list test (below):
+//  * a replica not cut into cells (CellGrid 1 x 1 x 1): every molecule of the
+//    replica is tested, 128 candidates at a time from shared memory (all lanes
+//    read the same candidate: a broadcast), which emits them in ascending j;
+//  * a replica cut into cells (k_replica_head): molecule i tests the molecules
+//    of its neighbouring cells only (their centres, sorted by cell, carry the
+//    local index in .w) and sets their bits in its row of a bitmap in shared
+//    memory (`win` words per row: molecules [32 w0, 32 (w0 + win)) at a time),
+//    then emits the set bits in ascending j -- the same list as the scan.
 // FP32 form: the skin list only has to contain every pair within rcut+skin
 // (pass 1 then keeps exactly the pairs within rcut), so the test is a
 // conservative one in FP32 on the top 16 bits of each fixed-point difference
@@ -262,76 +419,124 @@ struct ForceHead {
 // 1e-5.  It may keep a few pairs just beyond rcut+skin; the lists, and
 // therefore the results, of pass 1 do not change.
 template <int PREC>
+__device__ __forceinline__ bool list_test(const int4 me, const int4 cj, float lsc0, float lsc1, float lsc2,
+                                          float rl2f, double rx, double ry, double rz, const double* wj,
+                                          const double* L, double rl2) {
+  if (PREC == kF32) {
+    const float fx = (__int_as_float(0x4B400000 + (wrap_diff(me.x, cj.x) >> 16)) - 12582912.f) * lsc0;
+    const float fy = (__int_as_float(0x4B400000 + (wrap_diff(me.y, cj.y) >> 16)) - 12582912.f) * lsc1;
+    const float fz = (__int_as_float(0x4B400000 + (wrap_diff(me.z, cj.z) >> 16)) - 12582912.f) * lsc2;
+    return fx * fx + fy * fy + fz * fz < rl2f;
+  }
+  double dx = (rx - wj[0]) * L[0];
+  double dy = (ry - wj[1]) * L[1];
+  double dz = (rz - wj[2]) * L[2];
+  if (dx >= 0.5 * L[0]) dx -= L[0];
+  if (dx < -0.5 * L[0]) dx += L[0];
+  if (dy >= 0.5 * L[1]) dy -= L[1];
+  if (dy < -0.5 * L[1]) dy += L[1];
+  if (dz >= 0.5 * L[2]) dz -= L[2];
+  if (dz < -0.5 * L[2]) dz += L[2];
+  return dx * dx + dy * dy + dz * dz < rl2;
+}
+
+template <int PREC>
 __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
-                            uint16_t* nb, int tile_size) {
+                            uint16_t* nb, int tile_size, uint32_t* bm, int win) {
   __shared__ double4 cand[128];
   const int i = threadIdx.x;
   const bool valid = i < t.count;
   const int li = t.start + i;
   const double rl = c.rc + c.skin;
   const double rl2 = rl * rl;
-  int cnt = 0;
-  int ix = 0, iy = 0, iz = 0;
-  double rx = 0, ry = 0, rz = 0;
   const float lsc0 = (float)(L[0] * (1.0 / 65536.0)), lsc1 = (float)(L[1] * (1.0 / 65536.0)),
               lsc2 = (float)(L[2] * (1.0 / 65536.0));
   float rl2f = 0.f;
   if (PREC == kF32) {
-    const double lmax = fmax(fmax(L[0], L[1]), L[2]);
-    const double rw = (rl + 1.7320508075688772 * lmax * (1.0 / 65536.0)) * (1.0 + 1e-5);
+    const double rw = list_test_radius(c, L);
     rl2f = (float)(rw * rw);
   }
+  const int4* com = d.com + c.mol_off;
+  const double* pk = reinterpret_cast<const double*>(d.pack) + c.pack_off;
+  int4 me = make_int4(0, 0, 0, 0);
+  double rx = 0, ry = 0, rz = 0;
   if (valid) {
-    if (PREC == kF32) {
-      const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-      ix = w[0]; iy = w[1]; iz = w[2];
-    } else {
-      const double* w = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-      rx = w[0]; ry = w[1]; rz = w[2];
+    me = com[li];
+    if (PREC == kF64) {
+      rx = pk[(long long)li * c.pack_stride];
+      ry = pk[(long long)li * c.pack_stride + 1];
+      rz = pk[(long long)li * c.pack_stride + 2];
     }
   }
-  for (int base = 0; base < c.nmol; base += 128) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) {
-      const long long off = c.pack_off + (long long)(base + k) * c.pack_stride;
-      if (PREC == kF32) {
-        reinterpret_cast<int4*>(&cand[k])[0] = d.com[c.mol_off + base + k];
-      } else {
-        const double* w = reinterpret_cast<const double*>(d.pack) + off;
-        cand[k] = make_double4(w[0], w[1], w[2], 0);
-      }
-    }
-    __syncthreads();
-    if (valid) {
-      const int nk = min(128, c.nmol - base);
-      for (int k = 0; k < nk; k++) {
-        const int j = base + k;
+  const CellGrid g = d.cgrid[t.rep];
+  int cnt = 0;
+  if (g.nx * g.ny * g.nz == 1) {
+    // every molecule, 128 at a time through shared memory (uniform over the block)
+    for (int base = 0; base < c.nmol; base += 128) {
+      __syncthreads();
+      for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) {
         if (PREC == kF32) {
-          const int4 cj = reinterpret_cast<const int4*>(&cand[k])[0];
-          const float fx = (__int_as_float(0x4B400000 + (wrap_diff(ix, cj.x) >> 16)) - 12582912.f) * lsc0;
-          const float fy = (__int_as_float(0x4B400000 + (wrap_diff(iy, cj.y) >> 16)) - 12582912.f) * lsc1;
-          const float fz = (__int_as_float(0x4B400000 + (wrap_diff(iz, cj.z) >> 16)) - 12582912.f) * lsc2;
-          if (j != li && fx * fx + fy * fy + fz * fz < rl2f) {
+          reinterpret_cast<int4*>(&cand[k])[0] = com[base + k];
+        } else {
+          const double* w = pk + (long long)(base + k) * c.pack_stride;
+          cand[k] = make_double4(w[0], w[1], w[2], 0);
+        }
+      }
+      __syncthreads();
+      if (valid) {
+        const int nk = min(128, c.nmol - base);
+        for (int k = 0; k < nk; k++) {
+          const int j = base + k;
+          const bool in = list_test<PREC>(me, reinterpret_cast<const int4*>(&cand[k])[0], lsc0, lsc1, lsc2,
+                                          rl2f, rx, ry, rz, reinterpret_cast<const double*>(&cand[k]), L, rl2);
+          if (j != li && in) {
             if (cnt < c.nbr_cap) nb[(long long)cnt * tile_size] = (uint16_t)j;
             cnt++;
           }
-          continue;
         }
-        double dx, dy, dz;
-        {
-          const double4 cj = cand[k];
-          dx = (rx - cj.x) * L[0];
-          dy = (ry - cj.y) * L[1];
-          dz = (rz - cj.z) * L[2];
-          if (dx >= 0.5 * L[0]) dx -= L[0];
-          if (dx < -0.5 * L[0]) dx += L[0];
-          if (dy >= 0.5 * L[1]) dy -= L[1];
-          if (dy < -0.5 * L[1]) dy += L[1];
-          if (dz >= 0.5 * L[2]) dz -= L[2];
-          if (dz < -0.5 * L[2]) dz += L[2];
+      }
+    }
+  } else if (valid) {
+    uint32_t* row = bm + i * (win | 1);   // odd row length: the lanes' words fall in distinct banks
+    const int W = (c.nmol + 31) >> 5;
+    const int cx = cell_coord(me.x, g.nx), cy = cell_coord(me.y, g.ny), cz = cell_coord(me.z, g.nz);
+    const int ox = (g.nx == 1) ? 0 : 1, oy = (g.ny == 1) ? 0 : 1, oz = (g.nz == 1) ? 0 : 1;
+    const int* cs = d.cell_start + (long long)t.rep * (kMaxCells + 1);
+    const int4* cm = d.cell_com + c.mol_off;
+    for (int w0 = 0; w0 < W; w0 += win) {
+      const int nw = min(win, W - w0);
+      for (int w = 0; w < nw; w++) row[w] = 0u;
+      const int jlo = 32 * w0, jhi = 32 * (w0 + nw);
+      for (int dz = -oz; dz <= oz; dz++) {
+        int zc = cz + dz;
+        zc += (zc < 0) ? g.nz : 0;
+        zc -= (zc >= g.nz) ? g.nz : 0;
+        for (int dy = -oy; dy <= oy; dy++) {
+          int yc = cy + dy;
+          yc += (yc < 0) ? g.ny : 0;
+          yc -= (yc >= g.ny) ? g.ny : 0;
+          for (int dx = -ox; dx <= ox; dx++) {
+            int xc = cx + dx;
+            xc += (xc < 0) ? g.nx : 0;
+            xc -= (xc >= g.nx) ? g.nx : 0;
+            const int cell = (zc * g.ny + yc) * g.nx + xc;
+            const int e = cs[cell + 1];
+            for (int k = cs[cell]; k < e; k++) {
+              const int4 cj = cm[k];
+              const int j = cj.w;
+              if (j < jlo || j >= jhi || j == li) continue;
+              if (list_test<PREC>(me, cj, lsc0, lsc1, lsc2, rl2f, rx, ry, rz, pk + (long long)j * c.pack_stride,
+                                  L, rl2))
+                row[(j - jlo) >> 5] |= 1u << (j & 31);
+            }
+          }
         }
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        if (j != li && r2 < rl2) {
+      }
+      for (int w = 0; w < nw; w++) {
+        uint32_t bits = row[w];
+        while (bits) {
+          const int j = jlo + 32 * w + (__ffs(bits) - 1);
+          bits &= bits - 1u;
           if (cnt < c.nbr_cap) nb[(long long)cnt * tile_size] = (uint16_t)j;
           cnt++;
         }
@@ -857,11 +1062,10 @@ __device__ inline void zero_acc(IAcc& a) {
 // Skin-list rebuild of tile t when due, with the build's reference centres and box.
 template <int PREC>
 __device__ void rebuild_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
-                             uint16_t* nb, int tile_size) {
+                             uint16_t* nb, int tile_size, uint32_t* bm, int win) {
   const int i = threadIdx.x;
   const int li = t.start + i;
-  build_lists<PREC>(d, c, t, L, nb, tile_size);
-  __syncthreads();
+  build_lists<PREC>(d, c, t, L, nb, tile_size, bm, win);
   if (i < t.count) {
     int4 rc4;
     if (PREC == kF32) {
@@ -885,12 +1089,12 @@ __device__ inline bool site_image_needed(const RepConst& c, const double* L) {
 // FP64 form: rebuild when due, pair loop, wall, A2M.
 template <int S, int C0>
 __device__ void force_tile_f64(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
-                               bool rebuild, int tile_size) {
+                               bool rebuild, int tile_size, uint32_t* bm, int win) {
   const int i = threadIdx.x;
   const int li = t.start + i;
   const int g = c.mol_off + li;
   uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
-  if (rebuild) rebuild_tile<kF64>(d, c, t, tix, L, nb, tile_size);
+  if (rebuild) rebuild_tile<kF64>(d, c, t, tix, L, nb, tile_size, bm, win);
   IAcc a;
   zero_acc(a);
   double wall_e = 0.0;
@@ -970,84 +1174,45 @@ __device__ void force_tile_f32(const DevPtrs& d, const RepConst& c, const Tile& 
   write_part2(d, c, t, a, wall_e);
 }
 
-// Head of a force step (warp 0; lane 0 finishes): PsPv and D4 with the
-// integrate kernel's partials (src/integrator.cxx:132-172, 604-632), the
-// replica's new scalars to Xout (first tile), and whether this tile's skin
-// list must be rebuilt.  The partials are summed like reduce_part2 (lane-strided,
-// then a butterfly), so every tile of a replica gets the same bits.
-template <bool FORCE_ONLY>
-__device__ void force_head(const DevPtrs& d, const RepConst& c, int rep, int tix, const RepState* Yin,
-                           RepState* Xout, ForceHead& h) {
-  double v[4] = {0, 0, 0, 0}, disp = 0.0;
-  if (!FORCE_ONLY) {
-    for (int k = c.warp_off + (threadIdx.x & 31); k < c.warp_off + c.nwarp; k += 32) {
-      const Part1 p = d.part1[k];
-      v[0] += p.sum_Pv[0]; v[1] += p.sum_Pv[1]; v[2] += p.sum_Pv[2];
-      v[3] += p.sum_Ps;
-      disp = fmax(disp, p.disp);
-    }
-    warp_sum<4>(v);
-    disp = warp_max(disp);
-  }
-  if ((threadIdx.x & 31) != 0) return;
-  RepState st = Yin[rep];
-  if (!FORCE_ONLY) {
-    double sPv[3] = {v[0], v[1], v[2]};
-    const double sPs = v[3];
-    pspv(c, st, sPv, sPs);
-    d4(c, st);
-    if (tix == c.tile_off) Xout[rep] = st;
-    // list validity: pairs now within rc were within rc+skin at the build if
-    // 2*max|displacement| + rc*(max_d Lbuild_d/L_d - 1) <= skin
-    const double lb0 = d.Lbuild[3 * tix], lb1 = d.Lbuild[3 * tix + 1], lb2 = d.Lbuild[3 * tix + 2];
-    int rb = !(lb0 == lb0);
-    if (!rb) {
-      const double lam = fmax(fmax(lb0 / st.L[0], lb1 / st.L[1]), lb2 / st.L[2]);
-      rb = (2.0 * disp + c.rc * (lam - 1.0) > c.skin);
-    }
-    h.rebuild = rb;
-  } else {
-    h.rebuild = 1;
-  }
-  for (int x = 0; x < 3; x++) h.L[x] = st.L[x];
-}
-
-// FP64 form: one launch per step (head, rebuild, pairs, wall, A2M).
-template <bool FORCE_ONLY>
-__global__ void __launch_bounds__(128) k_force_f64(DevPtrs d, const RepState* __restrict__ Yin,
-                                                   RepState* __restrict__ Xout, int tile_size) {
-  __shared__ ForceHead h;
+// FP64 form: one launch per step after the replica head (list rebuild when
+// due, pairs, wall, A2M); the box and the rebuild decision come from
+// k_replica_head.
+__global__ void __launch_bounds__(128, 1) k_force_f64(DevPtrs d, const RepState* __restrict__ X, int tile_size) {
+  extern __shared__ uint32_t bm[];
+  __shared__ double Ls[3];
+  __shared__ int rb;
   const int tix = d.order ? d.order[blockIdx.x] : d.tile0 + blockIdx.x;   // costliest tiles first
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
-  if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
+  if (threadIdx.x < 3) Ls[threadIdx.x] = X[t.rep].L[threadIdx.x];
+  if (threadIdx.x == 0) rb = d.cgrid[t.rep].rebuild;
   __syncthreads();
-  const double L[3] = {h.L[0], h.L[1], h.L[2]};
-  const bool rb = h.rebuild != 0;
+  const double L[3] = {Ls[0], Ls[1], Ls[2]};
   if (c.nsite == 3)
-    force_tile_f64<3, 0>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<3, 0>(d, c, t, tix, L, rb != 0, tile_size, bm, d.bm_win);
   else if (c.nsite == 4)
-    force_tile_f64<4, 1>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<4, 1>(d, c, t, tix, L, rb != 0, tile_size, bm, d.bm_win);
   else
-    force_tile_f64<5, 1>(d, c, t, tix, L, rb, tile_size);
+    force_tile_f64<5, 1>(d, c, t, tix, L, rb != 0, tile_size, bm, d.bm_win);
 }
 
-// FP32 form, first launch of a step: head, skin-list rebuild when due, pass 1.
-// Light on registers, so many warps hide the gathered loads of pass 1.
-template <bool FORCE_ONLY>
-__global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepState* __restrict__ Yin,
-                                                     RepState* __restrict__ Xout, int tile_size) {
-  __shared__ ForceHead h;
+// FP32 form, first launch after the replica head: skin-list rebuild when due,
+// pass 1.  Light on registers, so many warps hide the gathered loads of pass 1.
+__global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepState* __restrict__ X, int tile_size) {
+  extern __shared__ uint32_t bm[];
+  __shared__ double Ls[3];
+  __shared__ int rb;
   const int tix = d.order ? d.order[blockIdx.x] : d.tile0 + blockIdx.x;
   const Tile t = d.tiles[tix];
   const RepConst& c = d.rc[t.rep];
-  if (threadIdx.x < 32) force_head<FORCE_ONLY>(d, c, t.rep, tix, Yin, Xout, h);
+  if (threadIdx.x < 3) Ls[threadIdx.x] = X[t.rep].L[threadIdx.x];
+  if (threadIdx.x == 0) rb = d.cgrid[t.rep].rebuild;
   __syncthreads();
-  const double L[3] = {h.L[0], h.L[1], h.L[2]};
+  const double L[3] = {Ls[0], Ls[1], Ls[2]};
   const int i = threadIdx.x;
   const int li = t.start + i;
   uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
-  if (h.rebuild) rebuild_tile<kF32>(d, c, t, tix, L, nb, tile_size);
+  if (rb) rebuild_tile<kF32>(d, c, t, tix, L, nb, tile_size, bm, d.bm_win);
   if (i < t.count) {
     uint16_t* nt = d.nbt + (nb - d.nbr);
     const int cnt = d.nbr_cnt[c.mol_off + li];
@@ -1076,7 +1241,6 @@ __global__ void __launch_bounds__(128, 3) k_force_pairs(DevPtrs d, const RepStat
 }
 
 // ------------------------------------------------------------------ per-replica kernels
-constexpr int kRepThreads = 256;
 
 __device__ inline double barostat_energy(const RepConst& c, const RepState& st) {
   // Molecules::BarostatEnergy (src/molecules.cxx:663-678); slit src/remdgpu.cu:2803-2809
@@ -1592,6 +1756,69 @@ void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double
   k_noalloc_store<<<1, 256, 0, s>>>(d, f_aos, n_aos, out);
 }
 
+// ------------------------------------------------------------------ carrying replicas between handles
+// The serving loop's batch changes: replicas that keep running are copied from
+// the previous handle's arrays into the new handle's, on the device.
+// src[k] = {first molecule of replica k in the old arrays, old replica} or -1.
+__global__ void k_carry_molecules(DevPtrs d, const double* __restrict__ r, const double* __restrict__ v,
+                                  const double* __restrict__ q, const double* __restrict__ p, int No,
+                                  const int2* __restrict__ src) {
+  const Tile t = d.tiles[blockIdx.x];
+  const int so = src[t.rep].x;
+  const int i = threadIdx.x;
+  if (so < 0 || i >= t.count) return;
+  const int li = t.start + i;
+  const int g = d.rc[t.rep].mol_off + li, go = so + li;
+  const int N = d.N;
+  for (int x = 0; x < 3; x++) {
+    d.r[x * N + g] = r[(long long)x * No + go];
+    d.v[x * N + g] = v[(long long)x * No + go];
+  }
+  for (int x = 0; x < 4; x++) {
+    d.q[x * N + g] = q[(long long)x * No + go];
+    d.p[x * N + g] = p[(long long)x * No + go];
+  }
+}
+
+// Per replica: the scalars and the pending condition; per ensemble (sens[e] =
+// old ensemble or -1): the exchange's slot -> replica index, interval counter
+// and seed.
+__global__ void k_carry_replicas(int nrep, int nens, RepState* __restrict__ X, const RepState* __restrict__ Xo,
+                                 double* __restrict__ T, double* __restrict__ P, const double* __restrict__ To,
+                                 const double* __restrict__ Po, const int2* __restrict__ src,
+                                 const int* __restrict__ sens, const int* __restrict__ rep_off,
+                                 const int* __restrict__ rep_off_o, const int* __restrict__ nrep_e,
+                                 int* __restrict__ index, const int* __restrict__ index_o,
+                                 long long* __restrict__ step, const long long* __restrict__ step_o,
+                                 unsigned long long* __restrict__ seed,
+                                 const unsigned long long* __restrict__ seed_o) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nrep; k += gridDim.x * blockDim.x) {
+    const int so = src[k].y;
+    if (so < 0) continue;
+    X[k] = Xo[so];
+    T[k] = To[so];
+    P[k] = Po[so];
+  }
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nens; e += gridDim.x * blockDim.x) {
+    const int eo = sens[e];
+    if (eo < 0) continue;
+    for (int c = 0; c < nrep_e[e]; c++) index[rep_off[e] + c] = index_o[rep_off_o[eo] + c];
+    step[e] = step_o[eo];
+    seed[e] = seed_o[eo];
+  }
+}
+
+void launch_carry(const DevPtrs& d, const DevPtrs& o, int tile, const int2* src, RepState* X, const RepState* Xo,
+                  double* T, double* P, const double* To, const double* Po, int nens, const int* sens,
+                  const int* rep_off, const int* rep_off_o, const int* nrep_e, int* index, const int* index_o,
+                  long long* step, const long long* step_o, unsigned long long* seed,
+                  const unsigned long long* seed_o, bool molecules, cudaStream_t s) {
+  if (molecules) k_carry_molecules<<<d.ntiles, tile, 0, s>>>(d, o.r, o.v, o.q, o.p, o.N, src);
+  k_carry_replicas<<<(std::max(d.nrep, nens) + 127) / 128, 128, 0, s>>>(
+      d.nrep, nens, X, Xo, T, P, To, Po, src, sens, rep_off, rep_off_o, nrep_e, index, index_o, step, step_o,
+      seed, seed_o);
+}
+
 // ------------------------------------------------------------------ launchers
 void launch_pack(const DevPtrs& d, int prec, int tile, cudaStream_t s) {
   k_pack<<<d.ntiles, tile, 0, s>>>(d, prec);
@@ -1607,23 +1834,35 @@ int max_force_tile(int prec) { return prec == kF32 ? 128 / kPairChunks : 128; }
 
 size_t force_smem_bytes(int tile) { return (size_t)(3 * kMaxSites + 8) * tile * sizeof(double); }
 
+// Bitmap of the list rebuild: one row of (win | 1) words per thread.
+size_t bitmap_smem_bytes(int tile, int win) { return (size_t)tile * (size_t)(win | 1) * sizeof(uint32_t); }
+
+int bitmap_window(int max_nmol) { return std::min((max_nmol + 31) / 32, kBitmapMaxWords); }
+
 cudaError_t force_kernel_setup() {
   // FP32 form: dynamic shared memory = the per-thread FP64 accumulators of a tile
   // of up to 128 molecules (23.5 KB, under the default limit; set explicitly so
-  // that a larger tile or more accumulators only change force_smem_bytes)
-  const int sm = (int)force_smem_bytes(128);
-  return cudaFuncSetAttribute(k_force_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  // that a larger tile or more accumulators only change force_smem_bytes); the
+  // list kernels' rebuild bitmaps (up to 128 rows of kBitmapMaxWords + 1 words)
+  cudaError_t e = cudaFuncSetAttribute(k_force_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)force_smem_bytes(128));
+  if (e != cudaSuccess) return e;
+  const int bms = (int)bitmap_smem_bytes(128, kBitmapMaxWords);
+  e = cudaFuncSetAttribute(k_force_lists, cudaFuncAttributeMaxDynamicSharedMemorySize, bms);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_force_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, bms);
 }
 
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s) {
+  if (force_only) k_replica_head<true><<<d.nrep_l, kRepThreads, 0, s>>>(d, Yin, Xout);
+  else k_replica_head<false><<<d.nrep_l, kRepThreads, 0, s>>>(d, Yin, Xout);
+  const size_t bms = bitmap_smem_bytes(tile, d.bm_win);
   if (prec == kF32) {
-    if (force_only) k_force_lists<true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
-    else k_force_lists<false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    k_force_lists<<<d.ntiles, tile, bms, s>>>(d, Xout, tile);
     k_force_pairs<<<d.ntiles, kPairChunks * tile, force_smem_bytes(kPairChunks * tile), s>>>(d, Xout, tile);
   } else {
-    if (force_only) k_force_f64<true><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
-    else k_force_f64<false><<<d.ntiles, tile, 0, s>>>(d, Yin, Xout, tile);
+    k_force_f64<<<d.ntiles, tile, bms, s>>>(d, Xout, tile);
   }
 }
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s) {

@@ -1,19 +1,23 @@
 // kernels.cuh -- the engine's CUDA kernels (sm_100a).
 //
-// One MD step of every replica of every ensemble is two launches over the same
-// tile grid (a tile = `blockDim.x` consecutive molecules of one replica):
+// One MD step of every replica of every ensemble is a short chain of launches
+// (a tile = `blockDim.x` consecutive molecules of one replica):
 //
-//   k_integrate  [end of the previous step: D5 kick, D5/D6 scalars]
-//                D6, D5, D4, D3 D2 D1 D2 D3 (src/integrator.cxx:646-673),
-//                then the force record of every molecule (fixed-point centre of
-//                mass + rotated site offsets) and the partial sums PsPv needs;
-//   k_force      PsPv + D4 (scalar chain), a neighbour-list rebuild when the
-//                skin criterion fails, the switched LJ + Coulomb pair loop,
-//                the wall, and the site -> molecule torque (A2M).
+//   k_integrate     [end of the previous step: D5 kick, D5/D6 scalars]
+//                   D6, D5, D4, D3 D2 D1 D2 D3 (src/integrator.cxx:646-673),
+//                   then the force record of every molecule (fixed-point centre
+//                   of mass + rotated site offsets) and the partial sums PsPv needs;
+//   k_replica_head  per replica: PsPv + D4 (scalar chain), the neighbour-list
+//                   decision and, when a rebuild is due, the cell lists;
+//   k_force_lists   per tile (FP32): the list rebuild from the cells when due,
+//                   then the per-step list of the pairs within rcut;
+//   k_force_pairs   per tile (FP32): the switched LJ + Coulomb pair loop, the
+//                   wall, and the site -> molecule torque (A2M);
+//   k_force_f64     per tile (FP64 form): rebuild, pair loop, wall, A2M.
 //
-// An interval is k_replica_start (exchange tail), interval x (k_integrate,
-// k_force), k_replica_end (last D5/D6 + CalcProperties -> Average), captured
-// once as a CUDA graph.
+// An interval is k_replica_start (exchange tail), interval x (step chain),
+// k_replica_end (last D5/D6 + CalcProperties -> Average), captured once as a
+// CUDA graph.
 #pragma once
 #include "engine_types.cuh"
 
@@ -29,6 +33,8 @@ void launch_integrate_prec(const DevPtrs& d, const RepState* X, RepState* Y, boo
 int max_force_tile(int prec);
 // Kernel attributes the force launches need (call once per device before launching).
 cudaError_t force_kernel_setup();
+// Words per row of the list-rebuild bitmap for replicas of up to max_nmol molecules (DevPtrs::bm_win).
+int bitmap_window(int max_nmol);
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s);
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s);
@@ -55,5 +61,13 @@ void launch_noalloc_load(const DevPtrs& d, const NoAllocSetup& setup, RepState* 
                          const double* q_aos, int tile, cudaStream_t s);
 void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s);
 int measure_fp32_fma(int device, double* ms, long long* flops);
+// Copies carried replicas from handle arrays `o` into `d` (serving batch changes):
+// molecule state (when `molecules`), RepState, pending condition, and per
+// carried ensemble the exchange index, counter and seed.
+void launch_carry(const DevPtrs& d, const DevPtrs& o, int tile, const int2* src, RepState* X, const RepState* Xo,
+                  double* T, double* P, const double* To, const double* Po, int nens, const int* sens,
+                  const int* rep_off, const int* rep_off_o, const int* nrep_e, int* index, const int* index_o,
+                  long long* step, const long long* step_o, unsigned long long* seed,
+                  const unsigned long long* seed_o, bool molecules, cudaStream_t s);
 
 }  // namespace remd

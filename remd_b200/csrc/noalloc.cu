@@ -7,9 +7,10 @@
 // cudaMalloc/cudaFree (both can synchronise the device).  They can still pass
 // in their own input and output buffers, but not give the engine its working
 // memory.  This entry point therefore keeps all of its scratch -- the
-// per-replica constants, the force records, the neighbour lists (skin and per-step), the partial
-// sums -- in one file-scope __device__ array of fixed size, which every GPU that
-// loads the library holds until the process exits.
+// per-replica constants, the force records, the cell and neighbour lists (skin
+// and per-step), the partial sums -- in one file-scope __device__ array of
+// fixed size, which every GPU that loads the library holds until the process
+// exits.
 //
 // Limits: at most kNoAllocMaxMol molecules (2048) and a neighbour capacity of
 // at most kNoAllocMaxNbr (1024) per molecule, i.e. rcut + 1 A skin <= ~13.4 A.
@@ -53,7 +54,10 @@ constexpr size_t kOffCom = kOffNtc + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffCnt = kOffCom + al(sizeof(int4) * kNoAllocMaxMol);
 constexpr size_t kOffPart = kOffCnt + al(4 * kNoAllocMaxMol);
 constexpr size_t kOffErr = kOffPart + al(sizeof(Part2) * (kNoAllocMaxMol / 32));
-constexpr size_t kScratchBytes = kOffErr + al(16);
+constexpr size_t kOffGrid = kOffErr + al(16);
+constexpr size_t kOffCellStart = kOffGrid + al(sizeof(CellGrid));
+constexpr size_t kOffCellMol = kOffCellStart + al(4 * (size_t)(kMaxCells + 1));
+constexpr size_t kScratchBytes = kOffCellMol + al(sizeof(int4) * (size_t)kNoAllocMaxMol);
 
 // The scratch itself.  On the host this name is only a stand-in for the
 // device array: host code must use the address from cudaGetSymbolAddress.
@@ -211,6 +215,12 @@ extern "C" remd_status remd_force_snapshot_noalloc(const remd_system_desc* s, co
   d.part2 = reinterpret_cast<Part2*>(b + kOffPart);
   d.err = reinterpret_cast<int*>(b + kOffErr);
   d.status = reinterpret_cast<int*>(b + kOffErr + 4);
+  d.cgrid = reinterpret_cast<CellGrid*>(b + kOffGrid);
+  d.cell_start = reinterpret_cast<int*>(b + kOffCellStart);
+  d.cell_com = reinterpret_cast<int4*>(b + kOffCellMol);
+  d.rep0 = 0;
+  d.nrep_l = 1;
+  d.bm_win = bitmap_window(s->nmol);
   RepState* X = reinterpret_cast<RepState*>(b + kOffState);
 
   // every earlier call's contents are overwritten before use: constants, tiles

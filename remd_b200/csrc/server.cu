@@ -3,17 +3,21 @@
 // A job is one REMD system (an ensemble: ntemp x npress replicas) to be run for
 // `ninterval` intervals (MD + Metropolis exchange each).  remd_server_step()
 // is one scheduling round:
-//   1. finished and cancelled jobs leave the batch, freeing their HBM;
+//   1. cancelled jobs leave the batch, freeing their HBM budget;
 //   2. queued jobs are admitted in arrival order while their estimated device
 //      footprint fits the budget (and their interval matches the batch's);
-//   3. if the batch changed, the running jobs' states are pulled from the
-//      device and one engine handle is built for the new set (state, H0,
-//      exchange index, step counter and seed carried over exactly);
+//   3. if the batch changed, a new engine handle is built for the new set: the
+//      jobs that keep running are copied into it from the previous handle on
+//      the device (molecule state, scalars and H0, pending conditions,
+//      exchange index, counter and seed), only new jobs' states come from the
+//      host; the handle's arrays come from a memory pool the server keeps, and
+//      its interval graph is the previous one updated in place;
 //   4. every job in the batch advances one interval in one graph launch.
 // Forces are a pure function of the positions (see pair_loop_f32) and every
 // per-replica reduction has a fixed order, so a job's trajectory is the same
 // bit for bit whether it runs alone or with any batch mates, and across batch
-// rebuilds (tests/test_gpu_server.py).
+// changes (tests/test_gpu_server.py).  A replica that goes non-finite or
+// overflows its neighbour list fails its own job only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,23 +32,24 @@
 #include "hostio.h"
 
 namespace remd {
-remd_status engine_set_h0(remd_handle h, const double* H0);
-remd_status engine_set_exchange(remd_handle h, const int* grids, const unsigned long long* seeds,
-                                const long long* steps, const int* index);
 remd_status engine_get_exchange(remd_handle h, long long* steps, int* index);
-remd_status engine_set_pending_conditions(remd_handle h, const double* T, const double* P);
 size_t engine_bytes(remd_handle h);
+remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
+                                const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
+                                const int* src_ens, const int* grids, const unsigned long long* seeds,
+                                const long long* steps, remd_precision prec, int device, cudaMemPool_t mempool,
+                                remd_handle* out);
 }  // namespace remd
 
 using namespace remd;
 
 namespace {
 
+// A replica's initial state, kept on the host from submission until the job
+// first joins a batch (afterwards its state lives on the device).
 struct Rep {
   std::vector<double> r, v, q, p, m, I;
-  double s, Ps, Q, Pv[3], W, L[3], T, P, H0;
-  double Tnext, Pnext;             // condition chosen by the last exchange, applied next interval
-  bool has_h0 = false;
+  double s, Ps, Q, Pv[3], W, L[3], T, P;
 };
 
 struct Job {
@@ -57,8 +62,10 @@ struct Job {
   remd_status status = REMD_OK;
   double t_submit = 0, t_start = 0, t_end = 0;
   std::vector<Rep> reps;
-  std::vector<int> index;          // condition slot -> replica
+  std::vector<int> index;          // condition slot -> replica (read back when the job leaves)
   long long step = 0;              // next exchange list type = step % 4
+  int ens_in_batch = -1;           // ensemble of the current batch handle, -1 before admission
+  int rep_in_batch = -1;           // its first replica there
   std::vector<double> avg;         // latest averages, nrep x 19
   size_t bytes = 0;
   int nrep() const { return nt * np; }
@@ -102,6 +109,7 @@ struct remd_server_s {
   std::vector<Job*> queue;         // waiting, in arrival order
   std::vector<Job*> active;        // in the current batch, in batch order
   remd_handle batch = nullptr;
+  cudaMemPool_t mempool = nullptr; // every batch handle's arrays (kept between batch changes)
   bool dirty = false;
   size_t in_use = 0;
   double t0 = now_s();
@@ -116,54 +124,42 @@ struct remd_server_s {
   }
 };
 
-static remd_status pull_batch(remd_server_s* S) {
+// The exchange index and interval counter of every job in the batch (a few
+// bytes per replica): read before a job leaves, for its result.
+static remd_status read_index(remd_server_s* S) {
   if (!S->batch) return REMD_OK;
-  int nens = (int)S->active.size();
-  std::vector<long long> steps(nens);
   int total = 0;
-  for (Job* j : S->active) total += j->nrep();
+  for (Job* j : S->active) total += j->nrep();   // every active job is in the batch here
+  std::vector<long long> steps(S->active.size());
   std::vector<int> idx(total);
   remd_status st = engine_get_exchange(S->batch, steps.data(), idx.data());
   if (st != REMD_OK) return st;
-  int rep = 0;
-  for (int e = 0; e < nens; e++) {
-    Job* j = S->active[e];
-    j->step = steps[e];
-    for (int k = 0; k < j->nrep(); k++, rep++) {
-      Rep& R = j->reps[k];
-      j->index[k] = idx[rep];
-      remd_state_view sv{};
-      sv.r = R.r.data(); sv.v = R.v.data(); sv.q = R.q.data(); sv.p = R.p.data();
-      if ((st = remd_get_state(S->batch, rep, &sv)) != REMD_OK) return st;
-      R.s = sv.s; R.Ps = sv.Ps;
-      for (int x = 0; x < 3; x++) { R.Pv[x] = sv.Pv[x]; R.L[x] = sv.L[x]; }
-      R.T = sv.T;
-      R.P = sv.P;
-      R.H0 = sv.H0;
-      R.has_h0 = true;
-    }
+  for (Job* j : S->active) {
+    j->step = steps[j->ens_in_batch];
+    j->index.assign(idx.begin() + j->rep_in_batch, idx.begin() + j->rep_in_batch + j->nrep());
   }
-  // the conditions the last exchange chose; applied (with the exchange tail) at
-  // the start of the replica's next interval
-  std::vector<double> T(total), P(total);
-  if ((st = remd_get_conditions(S->batch, nullptr, T.data(), P.data())) != REMD_OK) return st;
-  rep = 0;
-  for (Job* j : S->active)
-    for (int k = 0; k < j->nrep(); k++, rep++) { j->reps[k].Tnext = T[rep]; j->reps[k].Pnext = P[rep]; }
   return REMD_OK;
 }
 
+static void fill_init(const Rep& R, remd_replica_init& ri) {
+  ri.r = R.r.data(); ri.v = R.v.data(); ri.q = R.q.data(); ri.p = R.p.data();
+  ri.mass = R.m.data(); ri.inertia = R.I.data();
+  ri.s = R.s; ri.Ps = R.Ps; ri.Q = R.Q; ri.W = R.W; ri.T = R.T; ri.P = R.P;
+  for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
+}
+
+// A batch handle for the active jobs, continuing the previous one's.  On
+// failure the previous handle is left as it was.
 static remd_status build_batch(remd_server_s* S) {
-  if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
-  if (S->active.empty()) return REMD_OK;
+  if (S->active.empty()) {
+    if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
+    return REMD_OK;
+  }
   std::vector<remd_system_desc> sys;
-  std::vector<int> per;
+  std::vector<int> per, grids, src_rep, src_ens;
   std::vector<remd_replica_init> init;
-  std::vector<int> grids, index;
   std::vector<unsigned long long> seeds;
   std::vector<long long> steps;
-  std::vector<double> H0, Tnext, Pnext;
-  bool any_h0 = false;
   for (Job* j : S->active) {
     sys.push_back(j->sys);
     per.push_back(j->nrep());
@@ -171,52 +167,40 @@ static remd_status build_batch(remd_server_s* S) {
     grids.push_back(j->np);
     seeds.push_back(j->seed);
     steps.push_back(j->step);
+    src_ens.push_back(S->batch ? j->ens_in_batch : -1);
     for (int k = 0; k < j->nrep(); k++) {
-      const Rep& R = j->reps[k];
       remd_replica_init ri{};
-      ri.r = R.r.data(); ri.v = R.v.data(); ri.q = R.q.data(); ri.p = R.p.data();
-      ri.mass = R.m.data(); ri.inertia = R.I.data();
-      ri.s = R.s; ri.Ps = R.Ps; ri.Q = R.Q; ri.W = R.W; ri.T = R.T; ri.P = R.P;
-      for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
+      if (S->batch && j->ens_in_batch >= 0) {
+        src_rep.push_back(j->rep_in_batch + k);
+      } else {
+        src_rep.push_back(-1);
+        fill_init(j->reps[k], ri);
+      }
       init.push_back(ri);
-      index.push_back(j->index[k]);
-      H0.push_back(R.H0);
-      Tnext.push_back(R.Tnext);
-      Pnext.push_back(R.Pnext);
-      any_h0 = any_h0 || R.has_h0;
     }
   }
-  remd_status st = remd_create(sys.data(), (int)sys.size(), per.data(), init.data(), S->prec, S->device,
-                               &S->batch);
+  remd_handle nb = nullptr;
+  remd_status st = engine_create_carry(S->batch, sys.data(), (int)sys.size(), per.data(), init.data(),
+                                       src_rep.data(), src_ens.data(), grids.data(), seeds.data(), steps.data(),
+                                       S->prec, S->device, S->mempool, &nb);
   if (st != REMD_OK) return st;
-  if (any_h0) {
-    // a running job keeps its Hamiltonian reference; a new one takes the fresh value
-    std::vector<double> fresh(init.size());
-    int rep = 0;
-    for (Job* j : S->active)
-      for (int k = 0; k < j->nrep(); k++, rep++) {
-        remd_state_view sv{};
-        if ((st = remd_get_state(S->batch, rep, &sv)) != REMD_OK) return st;
-        fresh[rep] = j->reps[k].has_h0 ? j->reps[k].H0 : sv.H0;
-      }
-    if ((st = engine_set_h0(S->batch, fresh.data())) != REMD_OK) return st;
+  if (S->batch) remd_destroy(S->batch);
+  S->batch = nb;
+  int rep = 0;
+  for (size_t e = 0; e < S->active.size(); e++) {
+    Job* j = S->active[e];
+    j->ens_in_batch = (int)e;
+    j->rep_in_batch = rep;
+    rep += j->nrep();
+    std::vector<Rep>().swap(j->reps);   // its state lives on the device now
   }
-  if ((st = engine_set_pending_conditions(S->batch, Tnext.data(), Pnext.data())) != REMD_OK) return st;
-  return engine_set_exchange(S->batch, grids.data(), seeds.data(), steps.data(), index.data());
+  return REMD_OK;
 }
 
 // The status of building job j alone (its initial force call and H0).
 static remd_status job_alone_status(remd_server_s* S, Job* j) {
-  std::vector<remd_replica_init> init;
-  for (int k = 0; k < j->nrep(); k++) {
-    const Rep& R = j->reps[k];
-    remd_replica_init ri{};
-    ri.r = R.r.data(); ri.v = R.v.data(); ri.q = R.q.data(); ri.p = R.p.data();
-    ri.mass = R.m.data(); ri.inertia = R.I.data();
-    ri.s = R.s; ri.Ps = R.Ps; ri.Q = R.Q; ri.W = R.W; ri.T = R.T; ri.P = R.P;
-    for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
-    init.push_back(ri);
-  }
+  std::vector<remd_replica_init> init(j->nrep());
+  for (int k = 0; k < j->nrep(); k++) fill_init(j->reps[k], init[k]);
   const int per = j->nrep();
   remd_handle h = nullptr;
   const remd_status st = remd_create(&j->sys, 1, &per, init.data(), S->prec, S->device, &h);
@@ -237,10 +221,29 @@ remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision
     set_error("no CUDA device");
     return REMD_ERR_NO_DEVICE;
   }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    set_error("remd_server_open: bad device");
+    return REMD_ERR_INVALID;
+  }
+  // the batch handles' arrays: a pool that keeps what it has reserved, so that
+  // a batch change allocates without going back to the driver
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("remd_server_open: cannot create the device memory pool");
+    return REMD_ERR_CUDA;
+  }
+  unsigned long long keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   auto* S = new remd_server_s;
   S->budget = hbm_budget_bytes;
   S->device = device;
   S->prec = prec;
+  S->mempool = pool;
   *out = S;
   return REMD_OK;
 }
@@ -248,6 +251,10 @@ remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision
 remd_status remd_server_close(remd_server S) {
   if (!S) return REMD_OK;
   if (S->batch) remd_destroy(S->batch);
+  if (S->mempool) {
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(S->mempool);
+  }
   for (Job* j : S->jobs) delete j;
   delete S;
   return REMD_OK;
@@ -277,9 +284,7 @@ remd_status remd_job_submit(remd_server S, const remd_job_desc* jd, remd_job_id*
     R.r.assign(ri.r, ri.r + 3 * n); R.v.assign(ri.v, ri.v + 3 * n);
     R.q.assign(ri.q, ri.q + 4 * n); R.p.assign(ri.p, ri.p + 4 * n);
     R.m.assign(ri.mass, ri.mass + n); R.I.assign(ri.inertia, ri.inertia + 3 * n);
-    R.s = ri.s; R.Ps = ri.Ps; R.Q = ri.Q; R.W = ri.W; R.T = ri.T; R.P = ri.P; R.H0 = 0.0;
-    R.Tnext = ri.T;
-    R.Pnext = ri.P;
+    R.s = ri.s; R.Ps = ri.Ps; R.Q = ri.Q; R.W = ri.W; R.T = ri.T; R.P = ri.P;
     for (int x = 0; x < 3; x++) { R.Pv[x] = ri.Pv[x]; R.L[x] = ri.L[x]; }
     j->reps.push_back(R);
     j->index.push_back(k);
@@ -344,14 +349,11 @@ remd_status remd_job_result(remd_server S, remd_job_id id, double* averages, int
 remd_status remd_server_step(remd_server S, int* pending) {
   if (!S) return REMD_ERR_INVALID;
   std::lock_guard<std::mutex> lk(S->mu);
+  const double t_round = now_s();
   // 1. leave: cancelled jobs (finished ones left at the end of their last round)
   for (size_t e = 0; e < S->active.size();) {
     Job* j = S->active[e];
     if (j->state == 4) {
-      if (!S->dirty) {
-        remd_status st = pull_batch(S);
-        if (st != REMD_OK) return st;
-      }
       S->dirty = true;
       S->in_use -= j->bytes;
       j->t_end = now_s() - S->t0;
@@ -365,10 +367,6 @@ remd_status remd_server_step(remd_server S, int* pending) {
     Job* j = S->queue.front();
     if (!S->active.empty() && j->sys.interval != S->active[0]->sys.interval) break;
     if (S->in_use + j->bytes > S->budget) break;
-    if (!S->dirty && S->batch) {
-      remd_status st = pull_batch(S);
-      if (st != REMD_OK) return st;
-    }
     S->queue.erase(S->queue.begin());
     S->active.push_back(j);
     S->in_use += j->bytes;
@@ -376,17 +374,17 @@ remd_status remd_server_step(remd_server S, int* pending) {
     j->t_start = now_s() - S->t0;
     S->dirty = true;
   }
-  // 3. rebuild the batch handle if its membership changed
+  // 3. a new batch handle if the membership changed
   if (S->dirty) {
     remd_status st = build_batch(S);
     if (st != REMD_OK && st != REMD_ERR_CUDA) {
       // a job whose own state cannot start (e.g. a neighbour list over capacity
       // in the initial force call) fails alone: find it by building each job
-      // that has not run yet on its own, then rebuild without the failures
+      // that has not run yet on its own, then build again without the failures
       bool any = false;
       for (size_t e = 0; e < S->active.size();) {
         Job* j = S->active[e];
-        const remd_status sj = j->done == 0 ? job_alone_status(S, j) : REMD_OK;
+        const remd_status sj = j->ens_in_batch < 0 ? job_alone_status(S, j) : REMD_OK;
         if (sj != REMD_OK) {
           j->state = 3;
           j->status = sj;
@@ -401,10 +399,11 @@ remd_status remd_server_step(remd_server S, int* pending) {
       if (any) st = build_batch(S);
     }
     if (st != REMD_OK) {
-      for (Job* j : S->active) { j->state = 3; j->status = st; }
+      for (Job* j : S->active) { j->state = 3; j->status = st; j->t_end = now_s() - S->t0; }
       S->active.clear();
       S->in_use = 0;
       S->dirty = false;
+      if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
       return st;
     }
     S->dirty = false;
@@ -413,9 +412,7 @@ remd_status remd_server_step(remd_server S, int* pending) {
   if (S->batch) {
     const double t0 = now_s();
     remd_status st = remd_execute_steps_device(S->batch);
-    const double dt = now_s() - t0;
-    S->interval_ms.push_back(dt * 1e3);
-    S->busy_s += dt;
+    S->busy_s += now_s() - t0;
     S->intervals_done++;
     int total = 0;
     for (Job* j : S->active) total += j->nrep();
@@ -424,11 +421,11 @@ remd_status remd_server_step(remd_server S, int* pending) {
     // interval is complete and valid, and they keep running.
     std::vector<char> bad(S->active.size(), 0);
     if (st == REMD_ERR_NONFINITE || st == REMD_ERR_NEIGHBOR_OVERFLOW) {
-      int rep = 0, nbad = 0;
+      int nbad = 0;
       for (size_t e = 0; e < S->active.size(); e++)
-        for (int k = 0; k < S->active[e]->nrep(); k++, rep++) {
+        for (int k = 0; k < S->active[e]->nrep(); k++) {
           int w = 0;
-          if (remd_replica_status(S->batch, rep, &w) != REMD_OK) w = 1;
+          if (remd_replica_status(S->batch, S->active[e]->rep_in_batch + k, &w) != REMD_OK) w = 1;
           if (w != 0 && !bad[e]) { bad[e] = 1; nbad++; }
         }
       if (nbad > 0) {
@@ -455,7 +452,7 @@ remd_status remd_server_step(remd_server S, int* pending) {
       }
     }
     if (left) {
-      remd_status pst = pull_batch(S);   // final index/state of leaving jobs, carry-over of the rest
+      remd_status pst = read_index(S);   // the leaving jobs' final condition index
       if (pst != REMD_OK) return pst;
       for (size_t e = 0; e < S->active.size();) {
         Job* j = S->active[e];
@@ -470,6 +467,8 @@ remd_status remd_server_step(remd_server S, int* pending) {
         }
       }
     }
+    // the latency of the whole round: admission, any batch change and the interval
+    S->interval_ms.push_back((now_s() - t_round) * 1e3);
     if (st != REMD_OK) return st;
   }
   if (pending) *pending = (int)(S->queue.size() + S->active.size());

@@ -14,9 +14,10 @@ so every workload here is generated from a seed:
     VelocityScaling / KillMomentum / AngVelocityScaling (src/molecules.cxx:168-307)
     so every replica starts exactly at its condition's temperature.
 
-Periodic lengths follow from the lattice, not from the nominal lengths of the
-over-packed configurations; any periodic length below
-2*rcut+2 A is raised to that value so the minimum-image convention holds.
+Periodic lengths follow from the lattice (about 1.0 g/cm^3), not from the
+nominal lengths of configurations 1 and 2, which would pack water at about
+2.2x and 2.45x liquid density; any periodic length below 2*rcut+2 A is raised
+to that value so the minimum-image convention holds.
 """
 from __future__ import annotations
 

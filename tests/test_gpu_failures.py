@@ -90,6 +90,27 @@ def test_dense_job_fails_alone_in_the_server():
     srv.close()
 
 
+def test_dense_job_arriving_mid_run_fails_alone():
+    """The dense job joins a running batch: building the next batch handle fails
+    in its initial force call, the previous handle stays usable, the dense job
+    fails alone and the running job continues bit for bit."""
+    good = S.small_ensemble("tip5p", 1, nmol=100, ntemp=2, npress=2, seed=86, interval=10)
+    dense = _dense(S.small_ensemble("tip3p", 0, nmol=1000, ntemp=1, npress=1, seed=84, interval=10))
+    srv = E.Server(budget_bytes=8 << 30)
+    a = srv.submit(good, 4, seed=7)
+    srv.step()
+    srv.step()
+    b = srv.submit(dense, 2, seed=8)
+    while srv.step():
+        pass
+    assert srv.poll(b).state == 3 and srv.poll(b).status == 8
+    assert srv.poll(a).state == 2 and srv.poll(a).intervals_done == 4
+    avg, idx = srv.result(a, good.nreplica)
+    avg1, idx1 = _run_alone(good, 4, 7)
+    assert np.array_equal(avg, avg1) and np.array_equal(idx, idx1)
+    srv.close()
+
+
 def test_error_is_reported_once_then_cleared():
     """A histogram sample out of range is reported by the call that took it;
     the next interval, and an increment with a valid range, return REMD_OK."""

@@ -195,9 +195,10 @@ def test_velocity_scaling_in_a_mixed_batch():
     for prec in ["fp32", "fp64"]:
         mixed = E.REMDGPU([npt, vs], precision=prec)
         plain = E.REMDGPU([npt], precision=prec)
-        # per step: integrate, force (two launches in FP32), and for velocity scaling the
-        # rescale plus, after the first step, the closing kick; then start + end
-        per = 3 if prec == "fp32" else 2
+        # per step: integrate, replica head, force (two launches in FP32), and for
+        # velocity scaling the rescale plus, after the first step, the closing kick;
+        # then start + end
+        per = 4 if prec == "fp32" else 3
         assert mixed.launches_per_interval() == (per + 1) * NSTEPS + NSTEPS - 1 + 2
         T = np.concatenate([npt.T, vs.T])
         P = np.concatenate([npt.P, vs.P])
