@@ -67,7 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-serving", action="store_true",
                     help="config 4: skip the bounded serving sample (config 5's first --jobs jobs)")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
-    ap.add_argument("--study", choices=["drift", "lists"], default=None,
+    ap.add_argument("--study", choices=["drift", "lists", "clusters"], default=None,
                     help="drift: NP Hamiltonian drift of the precision-study system (config 3), "
                          "FP32 form on every replica and FP64 vs FP32 on a subset")
     ap.add_argument("--drift-ps", type=float, default=100.0, help="drift study length (ps)")
@@ -305,6 +305,7 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
     srv = E.Server(budget_bytes=budget, device=dev)
     n = len(jobs)
     ids, done_t, state = [None] * n, [None] * n, [0] * n
+    rounds = []   # (wall ms of one server round, molecule-steps of its interval)
     active = set()
     nxt = 0
     t0 = time.perf_counter()
@@ -320,7 +321,13 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
                 break
             time.sleep(max(arrivals[nxt] - now, 0.0))
             continue
+        # the round's work: one interval of every job that is queued or running
+        # (the server admits them all within the budget used here)
+        units_round = sum(jobs[k][0].spec.nmol * jobs[k][0].nreplica * jobs[k][0].spec.interval
+                          for k in active)
+        r0 = time.perf_counter()
         srv.step()
+        rounds.append(((time.perf_counter() - r0) * 1e3, units_round))
         now = time.perf_counter() - t0
         for k in sorted(active):
             st = srv.poll(ids[k]).state
@@ -337,7 +344,13 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
     return {"value": units / span, "makespan_s": span, "jobs_done": len(ok), "mol_steps": units,
             "p50_job_s": float(np.percentile(lat, 50)), "p99_job_s": float(np.percentile(lat, 99)),
             "p50_interval_ms": stats["p50_interval_ms"], "p99_interval_ms": stats["p99_interval_ms"],
-            "intervals": stats["intervals_done"], "busy_s": stats["busy_s"]}
+            "intervals": stats["intervals_done"], "busy_s": stats["busy_s"],
+            "batch_changes": stats["batch_changes"], "max_batch_change_ms": stats["max_batch_change_ms"],
+            "max_graph_ms": stats["max_graph_ms"],
+            # round time per million molecule-steps of its interval: the batch grows
+            # and shrinks as jobs come and go, which alone spreads the round times
+            "p50_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u in rounds], 50)),
+            "p99_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u in rounds], 99))}
 
 
 def serving_sample(seed, njobs, warmup, budget_gib, dev, world):
@@ -555,6 +568,71 @@ def lists_study(args, rank, world, local):
         for skin in (0.2, 1.0):
             measure(f"n4096_{model}_confined{confined}_skin{skin}", [e], skin, 30)
     print(json.dumps({"study": "lists", "unit": "ms per MD step", "systems": out}), flush=True)
+
+
+# ------------------------------------------------------------------ Newton's third law by cluster pairs (host)
+def _morton3(c):
+    """Z-order code of non-negative integer cell coordinates (n x 3, < 2^10)."""
+    code = np.zeros(len(c), dtype=np.int64)
+    for bit in range(10):
+        for d in range(3):
+            code |= ((c[:, d] >> bit) & 1).astype(np.int64) << (3 * bit + d)
+    return code
+
+
+def clusters_study(args, rank, world, local):
+    """How much pair work a Newton's-third-law scheme over spatial clusters of M
+    molecules would evaluate, against the engine's exact full lists, on the
+    config-4 systems (replica 0 of every ensemble, the seeded liquid-density
+    start).  Molecules are ordered along a Z-order curve of ~3.1 A cells and cut
+    into clusters of M consecutive molecules; a pair of clusters is evaluated
+    when their bounding boxes come within rcut (minimum image), every molecule
+    pair of it (M^2, or M(M-1)/2 on the diagonal) once.  The full lists evaluate
+    every pair within rcut twice (2U).  Host-only (numpy)."""
+    if rank != 0:
+        return
+    ens = workload(4, args.seed, args.interval)
+    out = {}
+    tot = {}
+    for e in ens:
+        st = e.states[0]
+        L = np.asarray(st.L, float)
+        x = (np.asarray(st.r, float) % 1.0) * L
+        n = len(x)
+        rc = e.spec.rcut
+        d = x[:, None, :] - x[None, :, :]
+        d -= L * np.round(d / L)
+        r2 = (d ** 2).sum(-1)
+        U = int(((r2 < rc * rc).sum() - n) // 2)
+        cell = np.floor(x / 3.1).astype(np.int64)
+        order = np.argsort(_morton3(cell), kind="stable")
+        row = {"nmol": n, "rcut": rc, "confined": e.spec.confined, "pairs_within_rc": U}
+        for M in (4, 8, 16, 32):
+            ids = [order[k:k + M] for k in range(0, n, M)]
+            cen, half = [], []
+            for c in ids:
+                p = x[c]
+                q = p - L * np.round((p - p[0]) / L)   # unwrap around the first member
+                lo, hi = q.min(0), q.max(0)
+                cen.append(0.5 * (lo + hi))
+                half.append(0.5 * (hi - lo))
+            cen, half = np.array(cen), np.array(half)
+            dc = cen[:, None, :] - cen[None, :, :]
+            dc -= L * np.round(dc / L)
+            gap = np.maximum(np.abs(dc) - (half[:, None, :] + half[None, :, :]), 0.0)
+            near = (gap ** 2).sum(-1) < rc * rc
+            sizes = np.array([len(c) for c in ids])
+            iu = np.triu_indices(len(ids), 1)
+            slots = int((sizes[iu[0]] * sizes[iu[1]])[near[iu]].sum() + (sizes * (sizes - 1) // 2).sum())
+            row[f"M{M}"] = {"slots": slots, "in_range_fraction": U / slots, "work_vs_full_lists": slots / (2 * U)}
+            t = tot.setdefault(M, [0, 0])
+            t[0] += slots
+            t[1] += 2 * U
+        out[e.name] = row
+    summary = {f"M{M}": {"work_vs_full_lists": s_ / u2, "in_range_fraction": u2 / 2 / s_}
+               for M, (s_, u2) in tot.items()}
+    print(json.dumps({"study": "clusters", "workload": "config 4, replica 0 of each ensemble (seeded start)",
+                      "summary": summary, "ensembles": out}), flush=True)
 
 
 # ------------------------------------------------------------------ engine arm
@@ -790,6 +868,10 @@ def engine_arm(args, rank, world, local):
                    "p50_interval_ms": sb["p50_interval_ms"], "p99_interval_ms": sb["p99_interval_ms"],
                    "p50_job_s": sb["p50_job_s"], "p99_job_s": sb["p99_job_s"],
                    "intervals": sb["intervals"], "jobs_done": sb["jobs_done"],
+                   "batch_changes": sb["batch_changes"], "max_batch_change_ms": sb["max_batch_change_ms"],
+                   "max_graph_ms": sb["max_graph_ms"],
+                   "p50_round_ms_per_Mmolstep": sb["p50_round_ms_per_Mmolstep"],
+                   "p99_round_ms_per_Mmolstep": sb["p99_round_ms_per_Mmolstep"],
                    "interval_latency": "wall time of one server round: admission, any batch change, "
                                        "the interval's graph launch and the averages' read-back"}
 
@@ -830,6 +912,8 @@ def main():
             drift_study(args, rank, world, local)
         elif args.study == "lists":
             lists_study(args, rank, world, local)
+        elif args.study == "clusters":
+            clusters_study(args, rank, world, local)
         elif args.config == 5:
             serving_arm(args, rank, world, local)
         else:

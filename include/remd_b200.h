@@ -369,10 +369,13 @@ typedef struct {
 
 typedef struct {
   long long jobs_done, intervals_done, mol_steps;
-  double p50_interval_ms, p99_interval_ms;   /* per batched interval */
-  double p50_job_s, p99_job_s;               /* submit -> done       */
+  double p50_interval_ms, p99_interval_ms;   /* per round: admission, batch change, interval */
+  double p50_job_s, p99_job_s;               /* submit -> done                               */
   double busy_s;
   long long bytes_in_use, budget_bytes;
+  long long batch_changes;                   /* rounds that built a new batch handle         */
+  double max_batch_change_ms;                /* slowest of those builds                      */
+  double max_graph_ms;                       /* slowest interval-graph capture + update      */
 } remd_server_stats;
 
 remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision prec,

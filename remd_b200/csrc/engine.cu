@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cmath>
 #include <cstring>
@@ -73,6 +74,7 @@ struct remd_engine_s {
   unsigned long long* d_seed = nullptr;   // per-ensemble Philox seed
   long long last_pairs = 0;
   long long steps_done = 0;        // MD steps run (the simulated time of the .chk Property line)
+  double last_graph_ms = 0.0;       // host time of the last interval-graph capture + update/instantiate
   cudaMemPool_t mempool = nullptr;  // the pool comes from this memory pool (serving loop), else cudaMalloc
   int pinned_cap = 0;               // replicas the pinned host buffers hold
   int2* d_carry_src = nullptr;      // per replica: {old first molecule, old replica} of a carried replica
@@ -497,6 +499,8 @@ remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
 }
 
 size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
+
+double engine_last_graph_ms(remd_handle h) { return h ? h->last_graph_ms : 0.0; }
 
 remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
                                 const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
@@ -991,8 +995,12 @@ remd_status remd_execute_steps_async(remd_handle h, const double* T, const doubl
   }
   if (!h->gexec || h->graph_tile != h->tile || h->graph_exchange != h->exch_enabled ||
       h->graph_hist != h->hist_on) {
+    const auto g0 = std::chrono::steady_clock::now();
     remd_status s = build_graph(h);
+    h->last_graph_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - g0).count();
     if (s != REMD_OK) return s;
+  } else {
+    h->last_graph_ms = 0.0;
   }
   CK(cudaGraphLaunch(h->gexec, h->stream));
   h->steps_done += h->interval;

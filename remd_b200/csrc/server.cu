@@ -34,6 +34,7 @@
 namespace remd {
 remd_status engine_get_exchange(remd_handle h, long long* steps, int* index);
 size_t engine_bytes(remd_handle h);
+double engine_last_graph_ms(remd_handle h);
 remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
                                 const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
                                 const int* src_ens, const int* grids, const unsigned long long* seeds,
@@ -116,6 +117,8 @@ struct remd_server_s {
   std::vector<double> interval_ms, job_s;
   long long jobs_done = 0, intervals_done = 0, mol_steps = 0;
   double busy_s = 0.0;
+  long long batch_changes = 0;
+  double max_change_ms = 0.0, max_graph_ms = 0.0;
 
   Job* find(remd_job_id id) {
     for (Job* j : jobs)
@@ -376,6 +379,7 @@ remd_status remd_server_step(remd_server S, int* pending) {
   }
   // 3. a new batch handle if the membership changed
   if (S->dirty) {
+    const double tb = now_s();
     remd_status st = build_batch(S);
     if (st != REMD_OK && st != REMD_ERR_CUDA) {
       // a job whose own state cannot start (e.g. a neighbour list over capacity
@@ -407,12 +411,15 @@ remd_status remd_server_step(remd_server S, int* pending) {
       return st;
     }
     S->dirty = false;
+    S->batch_changes++;
+    S->max_change_ms = std::max(S->max_change_ms, (now_s() - tb) * 1e3);
   }
   // 4. one interval (MD + exchange) for every running job
   if (S->batch) {
     const double t0 = now_s();
     remd_status st = remd_execute_steps_device(S->batch);
     S->busy_s += now_s() - t0;
+    S->max_graph_ms = std::max(S->max_graph_ms, engine_last_graph_ms(S->batch));
     S->intervals_done++;
     int total = 0;
     for (Job* j : S->active) total += j->nrep();
@@ -494,6 +501,9 @@ remd_status remd_server_stats_get(remd_server S, remd_server_stats* o) {
   o->busy_s = S->busy_s;
   o->bytes_in_use = (long long)S->in_use;
   o->budget_bytes = (long long)S->budget;
+  o->batch_changes = S->batch_changes;
+  o->max_batch_change_ms = S->max_change_ms;
+  o->max_graph_ms = S->max_graph_ms;
   return REMD_OK;
 }
 

@@ -175,7 +175,9 @@ class ServerStats(C.Structure):
                 ("mol_steps", C.c_longlong), ("p50_interval_ms", C.c_double),
                 ("p99_interval_ms", C.c_double), ("p50_job_s", C.c_double),
                 ("p99_job_s", C.c_double), ("busy_s", C.c_double),
-                ("bytes_in_use", C.c_longlong), ("budget_bytes", C.c_longlong)]
+                ("bytes_in_use", C.c_longlong), ("budget_bytes", C.c_longlong),
+                ("batch_changes", C.c_longlong), ("max_batch_change_ms", C.c_double),
+                ("max_graph_ms", C.c_double)]
 
 
 def _replica_inits(states):
