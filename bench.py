@@ -217,19 +217,22 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU baseline (reference)
-def cpu_baseline(ens, nsteps, nthreads):
-    """The reference's own CPU code (oracle/_ref generic FP64 build), every
-    replica advanced nsteps MD steps, replicas spread over nthreads host threads."""
+def cpu_baseline(ens, nsteps, nthreads, variant="generic"):
+    """The reference's own CPU code (oracle/_ref; by default the generic FP64
+    build, the one valid for every model and geometry), every replica advanced
+    nsteps MD steps, replicas spread over nthreads host threads."""
     from oracle import oracle as O
     kind = "reference"
-    if not O.reference_available():
+    if not O.reference_available(variant):
+        if variant != "generic":
+            return None
         kind = "port"
     refs = []
     t0 = time.perf_counter()
     for e in ens:
         for st in e.states:
             if kind == "reference":
-                r = O.Reference(e.spec, st, e.spec.moltype_file)
+                r = O.Reference(e.spec, st, e.spec.moltype_file, variant=variant)
                 r.initialize_property()
             else:
                 r = O.Oracle(e.spec, st)
@@ -248,7 +251,7 @@ def cpu_baseline(ens, nsteps, nthreads):
     dt = time.perf_counter() - t0
     return {"value": molsteps / dt, "unit": METRIC, "cores": cores, "kind": kind,
             "sample": f"all {len(refs)} replicas x {nsteps} MD steps "
-                      f"({'oracle/_ref generic FP64 build' if kind == 'reference' else 'C oracle'},"
+                      f"({'oracle/_ref ' + variant + ' build' if kind == 'reference' else 'C oracle'},"
                       f" replica-parallel over {cores} threads; {dt:.1f} s timed, setup {setup:.1f} s)",
             "seconds": dt}
 
@@ -880,6 +883,17 @@ def engine_arm(args, rank, world, local):
         nst = args.cpu_steps or 2
         cpu = cpu_baseline(ens, nst, cpu_threads())
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # config 1 (TIP4P nanotube) is the one workload the reference's tuned 4-site
+        # CPU path is valid for: also time it as shipped (makefile.gnu flags, FP32
+        # forces, replicas one after another) and as the tuned FP64 build
+        if args.config == 1:
+            forms = {}
+            for name, variant, threads in [("shipped_fp32_4site_serial", "shipped", 1),
+                                           ("tuned_fp64_4site_replica_parallel", "tuned4", cpu_threads())]:
+                r = cpu_baseline(ens, max(nst, 200), threads, variant)
+                if r:
+                    forms[name] = {k: r[k] for k in ("value", "unit", "cores", "sample")}
+            cpu["other_reference_forms"] = forms
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,

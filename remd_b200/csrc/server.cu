@@ -5,14 +5,16 @@
 // is one scheduling round:
 //   1. cancelled jobs leave the batch, freeing their HBM budget;
 //   2. queued jobs are admitted in arrival order while their estimated device
-//      footprint fits the budget (and their interval matches the batch's);
+//      footprint fits the budget, each into the batch of its MD interval length
+//      (jobs of different lengths run as separate batches, side by side);
 //   3. if the batch changed, a new engine handle is built for the new set: the
 //      jobs that keep running are copied into it from the previous handle on
 //      the device (molecule state, scalars and H0, pending conditions,
 //      exchange index, counter and seed), only new jobs' states come from the
 //      host; the handle's arrays come from a memory pool the server keeps, and
 //      its interval graph is the previous one updated in place;
-//   4. every job in the batch advances one interval in one graph launch.
+//   4. every job advances one interval: one graph launch per batch, the batches'
+//      graphs running at the same time on their own streams.
 // Forces are a pure function of the positions (see pair_loop_f32) and every
 // per-replica reduction has a fixed order, so a job's trajectory is the same
 // bit for bit whether it runs alone or with any batch mates, and across batch
@@ -100,6 +102,15 @@ double pct(std::vector<double> v, double q) {
 
 }  // namespace
 
+// The running jobs that share one MD interval length: one engine handle (one
+// interval graph) advances all of them by one interval per round.
+struct Batch {
+  int interval = 0;
+  std::vector<Job*> active;        // in batch order
+  remd_handle h = nullptr;
+  bool dirty = false;              // membership changed since h was built
+};
+
 struct remd_server_s {
   std::mutex mu;
   size_t budget = 0;
@@ -108,10 +119,8 @@ struct remd_server_s {
   remd_job_id next_id = 1;
   std::vector<Job*> jobs;          // every job ever submitted (owned)
   std::vector<Job*> queue;         // waiting, in arrival order
-  std::vector<Job*> active;        // in the current batch, in batch order
-  remd_handle batch = nullptr;
+  std::vector<Batch> batches;      // running jobs, one batch per MD interval length
   cudaMemPool_t mempool = nullptr; // every batch handle's arrays (kept between batch changes)
-  bool dirty = false;
   size_t in_use = 0;
   double t0 = now_s();
   std::vector<double> interval_ms, job_s;
@@ -129,15 +138,15 @@ struct remd_server_s {
 
 // The exchange index and interval counter of every job in the batch (a few
 // bytes per replica): read before a job leaves, for its result.
-static remd_status read_index(remd_server_s* S) {
-  if (!S->batch) return REMD_OK;
+static remd_status read_index(Batch& B) {
+  if (!B.h) return REMD_OK;
   int total = 0;
-  for (Job* j : S->active) total += j->nrep();   // every active job is in the batch here
-  std::vector<long long> steps(S->active.size());
+  for (Job* j : B.active) total += j->nrep();   // every active job is in the handle here
+  std::vector<long long> steps(B.active.size());
   std::vector<int> idx(total);
-  remd_status st = engine_get_exchange(S->batch, steps.data(), idx.data());
+  remd_status st = engine_get_exchange(B.h, steps.data(), idx.data());
   if (st != REMD_OK) return st;
-  for (Job* j : S->active) {
+  for (Job* j : B.active) {
     j->step = steps[j->ens_in_batch];
     j->index.assign(idx.begin() + j->rep_in_batch, idx.begin() + j->rep_in_batch + j->nrep());
   }
@@ -151,11 +160,11 @@ static void fill_init(const Rep& R, remd_replica_init& ri) {
   for (int x = 0; x < 3; x++) { ri.Pv[x] = R.Pv[x]; ri.L[x] = R.L[x]; }
 }
 
-// A batch handle for the active jobs, continuing the previous one's.  On
+// A batch handle for the batch's active jobs, continuing its previous one.  On
 // failure the previous handle is left as it was.
-static remd_status build_batch(remd_server_s* S) {
-  if (S->active.empty()) {
-    if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
+static remd_status build_batch(remd_server_s* S, Batch& B) {
+  if (B.active.empty()) {
+    if (B.h) { remd_destroy(B.h); B.h = nullptr; }
     return REMD_OK;
   }
   std::vector<remd_system_desc> sys;
@@ -163,17 +172,17 @@ static remd_status build_batch(remd_server_s* S) {
   std::vector<remd_replica_init> init;
   std::vector<unsigned long long> seeds;
   std::vector<long long> steps;
-  for (Job* j : S->active) {
+  for (Job* j : B.active) {
     sys.push_back(j->sys);
     per.push_back(j->nrep());
     grids.push_back(j->nt);
     grids.push_back(j->np);
     seeds.push_back(j->seed);
     steps.push_back(j->step);
-    src_ens.push_back(S->batch ? j->ens_in_batch : -1);
+    src_ens.push_back(B.h ? j->ens_in_batch : -1);
     for (int k = 0; k < j->nrep(); k++) {
       remd_replica_init ri{};
-      if (S->batch && j->ens_in_batch >= 0) {
+      if (B.h && j->ens_in_batch >= 0) {
         src_rep.push_back(j->rep_in_batch + k);
       } else {
         src_rep.push_back(-1);
@@ -183,15 +192,15 @@ static remd_status build_batch(remd_server_s* S) {
     }
   }
   remd_handle nb = nullptr;
-  remd_status st = engine_create_carry(S->batch, sys.data(), (int)sys.size(), per.data(), init.data(),
+  remd_status st = engine_create_carry(B.h, sys.data(), (int)sys.size(), per.data(), init.data(),
                                        src_rep.data(), src_ens.data(), grids.data(), seeds.data(), steps.data(),
                                        S->prec, S->device, S->mempool, &nb);
   if (st != REMD_OK) return st;
-  if (S->batch) remd_destroy(S->batch);
-  S->batch = nb;
+  if (B.h) remd_destroy(B.h);
+  B.h = nb;
   int rep = 0;
-  for (size_t e = 0; e < S->active.size(); e++) {
-    Job* j = S->active[e];
+  for (size_t e = 0; e < B.active.size(); e++) {
+    Job* j = B.active[e];
     j->ens_in_batch = (int)e;
     j->rep_in_batch = rep;
     rep += j->nrep();
@@ -253,7 +262,8 @@ remd_status remd_server_open(size_t hbm_budget_bytes, int device, remd_precision
 
 remd_status remd_server_close(remd_server S) {
   if (!S) return REMD_OK;
-  if (S->batch) remd_destroy(S->batch);
+  for (Batch& B : S->batches)
+    if (B.h) remd_destroy(B.h);
   if (S->mempool) {
     cudaDeviceSynchronize();
     cudaMemPoolDestroy(S->mempool);
@@ -349,137 +359,187 @@ remd_status remd_job_result(remd_server S, remd_job_id id, double* averages, int
   return REMD_OK;
 }
 
+// Builds the handle of a batch whose membership changed.  A job whose own
+// state cannot start (e.g. a neighbour list over capacity in the initial force
+// call) fails alone: it is found by building each job of the batch that has not
+// run yet on its own, and the batch is built again without the failures.
+static remd_status rebuild(remd_server_s* S, Batch& B) {
+  const double tb = now_s();
+  remd_status st = build_batch(S, B);
+  if (st != REMD_OK && st != REMD_ERR_CUDA) {
+    bool any = false;
+    for (size_t e = 0; e < B.active.size();) {
+      Job* j = B.active[e];
+      const remd_status sj = j->ens_in_batch < 0 ? job_alone_status(S, j) : REMD_OK;
+      if (sj != REMD_OK) {
+        j->state = 3;
+        j->status = sj;
+        j->t_end = now_s() - S->t0;
+        S->in_use -= j->bytes;
+        B.active.erase(B.active.begin() + e);
+        any = true;
+      } else {
+        e++;
+      }
+    }
+    if (any) st = build_batch(S, B);
+  }
+  if (st != REMD_OK) {
+    for (Job* j : B.active) {
+      j->state = 3;
+      j->status = st;
+      j->t_end = now_s() - S->t0;
+      S->in_use -= j->bytes;
+    }
+    B.active.clear();
+    if (B.h) { remd_destroy(B.h); B.h = nullptr; }
+  }
+  B.dirty = false;
+  S->batch_changes++;
+  S->max_change_ms = std::max(S->max_change_ms, (now_s() - tb) * 1e3);
+  return st;
+}
+
+// After an interval of batch B: the averages of every job, failures local to a
+// job, finished jobs leaving.  st is the interval's status.
+static remd_status collect(remd_server_s* S, Batch& B, remd_status st) {
+  int total = 0;
+  for (Job* j : B.active) total += j->nrep();
+  // A replica that went non-finite or overflowed its neighbour list fails its
+  // own job only: the replicas of the other jobs are independent of it, their
+  // interval is complete and valid, and they keep running.
+  std::vector<char> bad(B.active.size(), 0);
+  if (st == REMD_ERR_NONFINITE || st == REMD_ERR_NEIGHBOR_OVERFLOW) {
+    int nbad = 0;
+    for (size_t e = 0; e < B.active.size(); e++)
+      for (int k = 0; k < B.active[e]->nrep(); k++) {
+        int w = 0;
+        if (remd_replica_status(B.h, B.active[e]->rep_in_batch + k, &w) != REMD_OK) w = 1;
+        if (w != 0 && !bad[e]) { bad[e] = 1; nbad++; }
+      }
+    if (nbad > 0) {
+      for (size_t e = 0; e < B.active.size(); e++)
+        if (bad[e]) { B.active[e]->state = 3; B.active[e]->status = st; }
+      st = REMD_OK;
+    }
+  }
+  std::vector<double> avg((size_t)total * 19);
+  if (st == REMD_OK) st = remd_get_all_averages(B.h, avg.data());
+  int rep = 0;
+  bool left = false;
+  for (size_t e = 0; e < B.active.size(); e++) {
+    Job* j = B.active[e];
+    j->avg.assign(avg.begin() + (size_t)rep * 19, avg.begin() + (size_t)(rep + j->nrep()) * 19);
+    rep += j->nrep();
+    if (bad[e]) { left = true; continue; }
+    if (st != REMD_OK) { j->state = 3; j->status = st; left = true; continue; }
+    j->done++;
+    S->mol_steps += (long long)j->sys.nmol * j->nrep() * j->sys.interval;
+    if (j->done >= j->ninterval) {
+      j->state = 2;
+      left = true;
+    }
+  }
+  if (left) {
+    remd_status pst = read_index(B);   // the leaving jobs' final condition index
+    if (pst != REMD_OK) return pst;
+    for (size_t e = 0; e < B.active.size();) {
+      Job* j = B.active[e];
+      if (j->state == 2 || j->state == 3) {
+        j->t_end = now_s() - S->t0;
+        if (j->state == 2) { S->job_s.push_back(j->t_end - j->t_submit); S->jobs_done++; }
+        S->in_use -= j->bytes;
+        B.active.erase(B.active.begin() + e);
+        B.dirty = true;
+      } else {
+        e++;
+      }
+    }
+  }
+  return st;
+}
+
 remd_status remd_server_step(remd_server S, int* pending) {
   if (!S) return REMD_ERR_INVALID;
   std::lock_guard<std::mutex> lk(S->mu);
   const double t_round = now_s();
   // 1. leave: cancelled jobs (finished ones left at the end of their last round)
-  for (size_t e = 0; e < S->active.size();) {
-    Job* j = S->active[e];
-    if (j->state == 4) {
-      S->dirty = true;
-      S->in_use -= j->bytes;
-      j->t_end = now_s() - S->t0;
-      S->active.erase(S->active.begin() + e);
-    } else {
-      e++;
+  for (Batch& B : S->batches)
+    for (size_t e = 0; e < B.active.size();) {
+      Job* j = B.active[e];
+      if (j->state == 4) {
+        B.dirty = true;
+        S->in_use -= j->bytes;
+        j->t_end = now_s() - S->t0;
+        B.active.erase(B.active.begin() + e);
+      } else {
+        e++;
+      }
     }
-  }
-  // 2. admit in arrival order while the budget allows
+  // 2. admit in arrival order while the budget allows, each job into the batch
+  //    of its MD interval length
   while (!S->queue.empty()) {
     Job* j = S->queue.front();
-    if (!S->active.empty() && j->sys.interval != S->active[0]->sys.interval) break;
     if (S->in_use + j->bytes > S->budget) break;
     S->queue.erase(S->queue.begin());
-    S->active.push_back(j);
+    Batch* B = nullptr;
+    for (Batch& b : S->batches)
+      if (b.interval == j->sys.interval) B = &b;
+    if (!B) {
+      S->batches.emplace_back();
+      B = &S->batches.back();
+      B->interval = j->sys.interval;
+    }
+    B->active.push_back(j);
+    B->dirty = true;
     S->in_use += j->bytes;
     j->state = 1;
     j->t_start = now_s() - S->t0;
-    S->dirty = true;
   }
-  // 3. a new batch handle if the membership changed
-  if (S->dirty) {
-    const double tb = now_s();
-    remd_status st = build_batch(S);
-    if (st != REMD_OK && st != REMD_ERR_CUDA) {
-      // a job whose own state cannot start (e.g. a neighbour list over capacity
-      // in the initial force call) fails alone: find it by building each job
-      // that has not run yet on its own, then build again without the failures
-      bool any = false;
-      for (size_t e = 0; e < S->active.size();) {
-        Job* j = S->active[e];
-        const remd_status sj = j->ens_in_batch < 0 ? job_alone_status(S, j) : REMD_OK;
-        if (sj != REMD_OK) {
-          j->state = 3;
-          j->status = sj;
-          j->t_end = now_s() - S->t0;
-          S->in_use -= j->bytes;
-          S->active.erase(S->active.begin() + e);
-          any = true;
-        } else {
-          e++;
-        }
-      }
-      if (any) st = build_batch(S);
+  // 3. new handles for the batches whose membership changed
+  remd_status first_err = REMD_OK;
+  for (Batch& B : S->batches)
+    if (B.dirty) {
+      const remd_status st = rebuild(S, B);
+      if (st != REMD_OK && first_err == REMD_OK) first_err = st;
     }
-    if (st != REMD_OK) {
-      for (Job* j : S->active) { j->state = 3; j->status = st; j->t_end = now_s() - S->t0; }
-      S->active.clear();
-      S->in_use = 0;
-      S->dirty = false;
-      if (S->batch) { remd_destroy(S->batch); S->batch = nullptr; }
-      return st;
-    }
-    S->dirty = false;
-    S->batch_changes++;
-    S->max_change_ms = std::max(S->max_change_ms, (now_s() - tb) * 1e3);
+  // 4. one interval (MD + exchange) of every running job: the batches' graphs
+  //    are launched first, so that they run at the same time on their streams
+  bool ran = false;
+  std::vector<remd_status> launched(S->batches.size(), REMD_OK);
+  const double t0 = now_s();
+  for (size_t b = 0; b < S->batches.size(); b++)
+    if (S->batches[b].h) launched[b] = remd_execute_steps_async(S->batches[b].h, nullptr, nullptr);
+  for (size_t b = 0; b < S->batches.size(); b++) {
+    Batch& B = S->batches[b];
+    if (!B.h) continue;
+    remd_status st = launched[b];
+    if (st == REMD_OK) st = remd_synchronize(B.h);
+    S->max_graph_ms = std::max(S->max_graph_ms, engine_last_graph_ms(B.h));
+    ran = true;
+    st = collect(S, B, st);
+    if (st != REMD_OK && first_err == REMD_OK) first_err = st;
   }
-  // 4. one interval (MD + exchange) for every running job
-  if (S->batch) {
-    const double t0 = now_s();
-    remd_status st = remd_execute_steps_device(S->batch);
+  if (ran) {
     S->busy_s += now_s() - t0;
-    S->max_graph_ms = std::max(S->max_graph_ms, engine_last_graph_ms(S->batch));
     S->intervals_done++;
-    int total = 0;
-    for (Job* j : S->active) total += j->nrep();
-    // A replica that went non-finite or overflowed its neighbour list fails its
-    // own job only: the replicas of the other jobs are independent of it, their
-    // interval is complete and valid, and they keep running.
-    std::vector<char> bad(S->active.size(), 0);
-    if (st == REMD_ERR_NONFINITE || st == REMD_ERR_NEIGHBOR_OVERFLOW) {
-      int nbad = 0;
-      for (size_t e = 0; e < S->active.size(); e++)
-        for (int k = 0; k < S->active[e]->nrep(); k++) {
-          int w = 0;
-          if (remd_replica_status(S->batch, S->active[e]->rep_in_batch + k, &w) != REMD_OK) w = 1;
-          if (w != 0 && !bad[e]) { bad[e] = 1; nbad++; }
-        }
-      if (nbad > 0) {
-        for (size_t e = 0; e < S->active.size(); e++)
-          if (bad[e]) { S->active[e]->state = 3; S->active[e]->status = st; }
-        st = REMD_OK;
-      }
-    }
-    std::vector<double> avg((size_t)total * 19);
-    if (st == REMD_OK) st = remd_get_all_averages(S->batch, avg.data());
-    int rep = 0;
-    bool left = false;
-    for (size_t e = 0; e < S->active.size(); e++) {
-      Job* j = S->active[e];
-      j->avg.assign(avg.begin() + (size_t)rep * 19, avg.begin() + (size_t)(rep + j->nrep()) * 19);
-      rep += j->nrep();
-      if (bad[e]) { left = true; continue; }
-      if (st != REMD_OK) { j->state = 3; j->status = st; left = true; continue; }
-      j->done++;
-      S->mol_steps += (long long)j->sys.nmol * j->nrep() * j->sys.interval;
-      if (j->done >= j->ninterval) {
-        j->state = 2;
-        left = true;
-      }
-    }
-    if (left) {
-      remd_status pst = read_index(S);   // the leaving jobs' final condition index
-      if (pst != REMD_OK) return pst;
-      for (size_t e = 0; e < S->active.size();) {
-        Job* j = S->active[e];
-        if (j->state == 2 || j->state == 3) {
-          j->t_end = now_s() - S->t0;
-          if (j->state == 2) { S->job_s.push_back(j->t_end - j->t_submit); S->jobs_done++; }
-          S->in_use -= j->bytes;
-          S->active.erase(S->active.begin() + e);
-          S->dirty = true;
-        } else {
-          e++;
-        }
-      }
-    }
     // the latency of the whole round: admission, any batch change and the interval
     S->interval_ms.push_back((now_s() - t_round) * 1e3);
-    if (st != REMD_OK) return st;
   }
-  if (pending) *pending = (int)(S->queue.size() + S->active.size());
-  return REMD_OK;
+  // batches left without jobs release their handles
+  for (size_t b = 0; b < S->batches.size();) {
+    Batch& B = S->batches[b];
+    if (B.active.empty()) {
+      if (B.h) remd_destroy(B.h);
+      S->batches.erase(S->batches.begin() + b);
+    } else {
+      b++;
+    }
+  }
+  size_t running = 0;
+  for (const Batch& B : S->batches) running += B.active.size();
+  if (pending) *pending = (int)(S->queue.size() + running);
+  return first_err;
 }
 
 remd_status remd_job_bytes(const remd_job_desc* jd, size_t* out) {

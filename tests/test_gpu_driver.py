@@ -112,3 +112,19 @@ def test_reference_remd_driver_runs_on_the_engine(tmp_path):
     cdv = open(out / "gpuR0000s0000000.cdv").read().splitlines()
     assert cdv[0].startswith("' box_sx=-7.4 box_sy=-7.4 ") and 'st0="T=200 K, P=4000 MPa"' in cdv[0]
     assert len(cdv) == 601 and cdv[1].split()[:2] == ["0", "0"] and cdv[600].split()[:2] == ["149", "3"]
+    # the end-of-run files of REMD::ExecuteREMD (src/remd.cxx:448-460):
+    # energy.dat (REMD::OutputEnergy, src/remd.cxx:838-849): the step, then per replica
+    # the last interval's potential plus volume x pressure (barostat on), 16 digits
+    last = np.array(rows[-1][3:5], dtype=float)   # pot, vol of interval 1 (6 digits)
+    ene = open(out / "energy.dat").read().split()
+    assert int(ene[0]) == 2 and len(ene) == 2
+    assert float(ene[1]) == pytest.approx(last[0] + last[1] * P, rel=1e-5)
+    # index_temp.dat / index_press.dat (REMD::OutputIndex, src/remd.cxx:851-879)
+    it = open(out / "index_temp.dat").read().split()
+    ip = open(out / "index_press.dat").read().split()
+    assert int(it[0]) == 2 and int(ip[0]) == 2
+    assert float(it[1]) == pytest.approx(T, abs=1e-6) and float(ip[1]) == pytest.approx(P, abs=1e-6)
+    # accept_rate.dat and tunnel_count.dat (REMDInfo, src/remdinfo.cxx:762-832): one
+    # condition, so no exchange pair and one tunnel counter
+    assert open(out / "accept_rate.dat").read().startswith("#Ti,Pi,Tj,Pj,AR\n")
+    assert len(open(out / "tunnel_count.dat").read().split()) == 1

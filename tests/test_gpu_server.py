@@ -75,3 +75,25 @@ def test_budget_admission_and_cancel():
     st = srv.stats()
     assert st["bytes_in_use"] == 0 and st["jobs_done"] == 2
     srv.close()
+
+
+def test_jobs_of_different_interval_lengths_run_side_by_side():
+    """Jobs whose MD interval lengths differ run as separate batches in the same
+    rounds (their graphs side by side on their own streams); each result still
+    equals the job run alone, bit for bit."""
+    a = S.small_ensemble("tip4p", 0, nmol=80, ntemp=2, npress=1, seed=91, interval=10)
+    b = S.small_ensemble("tip3p", 1, nmol=96, ntemp=2, npress=2, seed=92, interval=5)
+    c = S.small_ensemble("tip5p", 2, nmol=90, ntemp=2, npress=1, seed=93, interval=10)
+    srv = E.Server(budget_bytes=8 << 30)
+    ids = [srv.submit(a, 3, seed=11), srv.submit(b, 4, seed=12)]
+    srv.step()
+    assert srv.poll(ids[0]).state == 1 and srv.poll(ids[1]).state == 1   # both running
+    ids.append(srv.submit(c, 2, seed=13))
+    while srv.step():
+        pass
+    for e, jid, n, seed in zip([a, b, c], ids, [3, 4, 2], [11, 12, 13]):
+        assert srv.poll(jid).state == 2 and srv.poll(jid).intervals_done == n
+        avg, idx = srv.result(jid, e.nreplica)
+        avg1, idx1 = _alone(e, n, seed)
+        assert np.array_equal(avg, avg1) and np.array_equal(idx, idx1)
+    srv.close()
