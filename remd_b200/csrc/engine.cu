@@ -8,10 +8,15 @@
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <iomanip>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/remd_b200.h"
@@ -89,6 +94,40 @@ struct remd_engine_s {
   bool hist_on = false;             // some ensemble keeps a histogram
   bool graph_hist = false;
 };
+
+// Wall tables by their parameters.  The tube table integrates over the wall
+// once per entry (about a second of host time for 65536 entries), and a
+// serving batch is rebuilt whenever a job joins or leaves it; the tables of the
+// jobs still running come from here instead of being computed again.  The
+// cache keeps the most recent kWallCacheMax tables (1 MB each at 65536 entries).
+using WallKey = std::tuple<int, int, double, double, double, double>;
+static WallKey wall_key(const remd_system_desc& s) {
+  return WallKey(s.confined, s.nfwall, s.wall_length, s.sgm_wall, s.eps_wall, s.rho_wall);
+}
+constexpr size_t kWallCacheMax = 64;
+static std::mutex g_wall_mu;
+static std::map<WallKey, std::shared_ptr<const std::vector<double>>> g_wall_cache;
+static std::deque<WallKey> g_wall_order;   // oldest first
+
+static std::shared_ptr<const std::vector<double>> wall_table_cached(const remd_system_desc& s) {
+  const WallKey k = wall_key(s);
+  {
+    std::lock_guard<std::mutex> g(g_wall_mu);
+    auto it = g_wall_cache.find(k);
+    if (it != g_wall_cache.end()) return it->second;
+  }
+  auto t = std::make_shared<std::vector<double>>(2 * (size_t)s.nfwall);
+  wall_table(s.confined, s.nfwall, s.wall_length, s.sgm_wall, s.eps_wall, s.rho_wall, t->data());
+  std::lock_guard<std::mutex> g(g_wall_mu);
+  if (g_wall_cache.emplace(k, t).second) {
+    g_wall_order.push_back(k);
+    if (g_wall_order.size() > kWallCacheMax) {
+      g_wall_cache.erase(g_wall_order.front());
+      g_wall_order.pop_front();
+    }
+  }
+  return t;
+}
 
 static int valid_model(const remd_system_desc& s, int* c0) {
   const int ns = s.nsite;
@@ -625,16 +664,19 @@ static remd_status create_impl(const remd_system_desc* systems, int nens, const 
   h->nens = nens;
   h->interval = systems[0].interval;
   h->sys.assign(systems, systems + nens);
-  // wall tables, one per ensemble
+  // wall tables: one per distinct set of wall parameters, shared by the
+  // ensembles that have it
   std::vector<int> wall_off(nens, 0);
   for (int e = 0; e < nens; e++) {
     const remd_system_desc& s = systems[e];
-    if (s.confined > 0) {
-      wall_off[e] = (int)(h->wall_h.size() / 2);
-      std::vector<double> t(2 * (size_t)s.nfwall);
-      wall_table(s.confined, s.nfwall, s.wall_length, s.sgm_wall, s.eps_wall, s.rho_wall, t.data());
-      h->wall_h.insert(h->wall_h.end(), t.begin(), t.end());
-    }
+    if (s.confined <= 0) continue;
+    int same = -1;
+    for (int f = 0; f < e && same < 0; f++)
+      if (wall_key(systems[f]) == wall_key(s)) same = f;
+    if (same >= 0) { wall_off[e] = wall_off[same]; continue; }
+    wall_off[e] = (int)(h->wall_h.size() / 2);
+    const auto t = wall_table_cached(s);
+    h->wall_h.insert(h->wall_h.end(), t->begin(), t->end());
   }
   // replicas
   int rep = 0, mol = 0;

@@ -15,6 +15,7 @@ namespace remd {
 constexpr int kRepThreads = 256;   // threads of the per-replica kernels
 constexpr int kBitmapMaxWords = 64; // list-rebuild bitmap window: 2048 molecules per pass
 constexpr int kCellMinPrune = 4;    // cut a replica into cells when they prune at least 4x
+constexpr int kListLanes = 4;       // lanes per molecule in the FP32 list kernel (adjacent in a warp)
 
 int pack_stride(int nsite, int prec) {
   if (prec == kF32) return ((3 + 3 * nsite) + 3) / 4 * 4;   // words, 16-B multiple
@@ -298,6 +299,11 @@ __device__ inline CellGrid cell_grid(const RepConst& c, const double* L) {
   return g;
 }
 
+// The kListLanes bits of a warp ballot that belong to this lane's molecule.
+__device__ __forceinline__ unsigned group_bits(unsigned ballot, int lane) {
+  return (ballot >> (lane & ~(kListLanes - 1))) & ((1u << kListLanes) - 1u);
+}
+
 __device__ inline int cell_of(const int4 x, const CellGrid& g) {
   return (cell_coord(x.z, g.nz) * g.ny + cell_coord(x.y, g.ny)) * g.nx + cell_coord(x.x, g.nx);
 }
@@ -553,6 +559,122 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
   }
 }
 
+// FP32 skin-list build for the list kernel, kListLanes lanes per molecule
+// (molecule slot threadIdx.x / kListLanes, lane sub = threadIdx.x % kListLanes).
+// The lists are those of build_lists<kF32>, entry for entry:
+//  * all-molecule scan: lane sub tests candidates sub, sub + 4, ... of each
+//    128-molecule chunk staged in shared memory, and a ballot places the kept
+//    ones in ascending j;
+//  * cell lists: the lanes split each neighbouring cell's molecules and set
+//    the molecule's bitmap row with shared-memory atomics; the row is then
+//    emitted in ascending j, lane sub taking words sub, sub + 4, ..., placed by
+//    a prefix of their popcounts over the group.
+// Returns the list length (equal on the group's lanes); lane 0 stores it.
+__device__ int build_lists_f32(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
+                               uint16_t* nb, int T, uint32_t* bm, int win) {
+  __shared__ int4 cand[128];
+  const int i = threadIdx.x / kListLanes, sub = threadIdx.x % kListLanes, lane = threadIdx.x & 31;
+  const unsigned below = (1u << sub) - 1u;
+  const bool valid = i < t.count;
+  const int li = t.start + i;
+  const float lsc0 = (float)(L[0] * (1.0 / 65536.0)), lsc1 = (float)(L[1] * (1.0 / 65536.0)),
+              lsc2 = (float)(L[2] * (1.0 / 65536.0));
+  const double rw = list_test_radius(c, L);
+  const float rl2f = (float)(rw * rw);
+  const int4* com = d.com + c.mol_off;
+  const int4 me = valid ? com[li] : make_int4(0, 0, 0, 0);
+  const CellGrid g = d.cgrid[t.rep];
+  int cnt = 0;
+  if (g.nx * g.ny * g.nz == 1) {
+    for (int base = 0; base < c.nmol; base += 128) {   // uniform over the block
+      __syncthreads();
+      for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) cand[k] = com[base + k];
+      __syncthreads();
+      const int nk = min(128, c.nmol - base);
+      for (int k0 = 0; k0 < nk; k0 += kListLanes) {
+        const int k = k0 + sub, j = base + k;
+        const bool in = valid && k < nk && j != li &&
+                        list_test<kF32>(me, cand[k], lsc0, lsc1, lsc2, rl2f, 0.0, 0.0, 0.0, nullptr, L, 0.0);
+        const unsigned gb = group_bits(__ballot_sync(0xffffffffu, in), lane);
+        if (in) {
+          const int pos = cnt + __popc(gb & below);
+          if (pos < c.nbr_cap) nb[(long long)pos * T] = (uint16_t)j;
+        }
+        cnt += __popc(gb);
+      }
+    }
+  } else {
+    uint32_t* row = bm + i * (win | 1);   // odd row length: the molecules' words fall in distinct banks
+    const int W = (c.nmol + 31) >> 5;
+    const int cx = cell_coord(me.x, g.nx), cy = cell_coord(me.y, g.ny), cz = cell_coord(me.z, g.nz);
+    const int ox = (g.nx == 1) ? 0 : 1, oy = (g.ny == 1) ? 0 : 1, oz = (g.nz == 1) ? 0 : 1;
+    const int* cs = d.cell_start + (long long)t.rep * (kMaxCells + 1);
+    const int4* cm = d.cell_com + c.mol_off;
+    for (int w0 = 0; w0 < W; w0 += win) {   // uniform over the block
+      const int nw = min(win, W - w0);
+      for (int w = sub; w < nw; w += kListLanes) row[w] = 0u;
+      __syncwarp();
+      const int jlo = 32 * w0, jhi = 32 * (w0 + nw);
+      if (valid) {
+        for (int dz = -oz; dz <= oz; dz++) {
+          int zc = cz + dz;
+          zc += (zc < 0) ? g.nz : 0;
+          zc -= (zc >= g.nz) ? g.nz : 0;
+          for (int dy = -oy; dy <= oy; dy++) {
+            int yc = cy + dy;
+            yc += (yc < 0) ? g.ny : 0;
+            yc -= (yc >= g.ny) ? g.ny : 0;
+            for (int dx = -ox; dx <= ox; dx++) {
+              int xc = cx + dx;
+              xc += (xc < 0) ? g.nx : 0;
+              xc -= (xc >= g.nx) ? g.nx : 0;
+              const int cell = (zc * g.ny + yc) * g.nx + xc;
+              const int e = cs[cell + 1];
+              for (int k = cs[cell] + sub; k < e; k += kListLanes) {
+                const int4 cj = cm[k];
+                const int j = cj.w;
+                if (j < jlo || j >= jhi || j == li) continue;
+                if (list_test<kF32>(me, cj, lsc0, lsc1, lsc2, rl2f, 0.0, 0.0, 0.0, nullptr, L, 0.0))
+                  atomicOr(&row[(j - jlo) >> 5], 1u << (j & 31));
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();
+      for (int w = 0; w < nw; w += kListLanes) {   // uniform over the block
+        const uint32_t word = (w + sub < nw) ? row[w + sub] : 0u;
+        const int n = __popc(word);
+        int incl = n;   // inclusive prefix of n over the group's lanes
+#pragma unroll
+        for (int o = 1; o < kListLanes; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o, kListLanes);
+          if (sub >= o) incl += y;
+        }
+        int pos = cnt + incl - n;
+        uint32_t bits = word;
+        while (bits) {
+          const int j = jlo + 32 * (w + sub) + (__ffs(bits) - 1);
+          bits &= bits - 1u;
+          if (pos < c.nbr_cap) nb[(long long)pos * T] = (uint16_t)j;
+          pos++;
+        }
+        cnt += __shfl_sync(0xffffffffu, incl, kListLanes - 1, kListLanes);
+      }
+      __syncwarp();   // the row is cleared again for the next window
+    }
+  }
+  if (cnt > c.nbr_cap) {
+    if (valid && sub == 0) {
+      atomicOr(d.err, kErrNbrOverflow);
+      atomicMax(&d.status[t.rep], 8);
+    }
+    cnt = c.nbr_cap;
+  }
+  if (valid && sub == 0) d.nbr_cnt[c.mol_off + li] = cnt;
+  return cnt;
+}
+
 // Accumulators of one molecule i.
 struct IAcc {
   double fs[kMaxSites][3];   // site forces (switched pair terms + wall on site 0)
@@ -670,19 +792,22 @@ __device__ __noinline__ void site_pair_exact(const DevPtrs& d, const RepConst& c
   acc[(3 * S + 7) * T + tid] += (double)(sw * ecl);
 }
 
-// Pass 1 for molecule li of tile t: the neighbours of its (rcut + skin) list
-// that are within rcut, in ascending j, into its column of `nt` -- far pairs
-// from the front, near pairs (SIMG only) from the back -- eight candidates per
-// round so that their record loads are in flight together.  Stores
-// nfar | nnear << 16 in d.nt_cnt.
+// Pass 1 for molecule li of tile t, run by its kListLanes lanes (sub = 0..3):
+// the neighbours of its (rcut + skin) list that are within rcut, in ascending
+// j, into its column of `nt` -- far pairs from the front, near pairs (SIMG
+// only) from the back.  Lane sub tests list entries sub, sub + 4, ...; a round
+// of the group covers four consecutive entries, and the kept ones are placed by
+// a ballot in list order, so the lists equal those of one lane walking the
+// list in turn.  Four rounds per batch, so that their record loads are in
+// flight together.  Lane 0 stores nfar | nnear << 16 in d.nt_cnt.  Every lane
+// of the warp runs the warp's longest list (ballots need the whole warp).
 template <bool SIMG>
-__device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, const double* L,
-                                const uint16_t* nb, uint16_t* nt, int cnt) {
-  const int T = blockDim.x;
+__device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, bool valid, int sub,
+                                const double* L, const uint16_t* nb, uint16_t* nt, int cnt, int T) {
   const int4* base = d.com + c.mol_off;   // compact centres: 16 B per molecule, L1-resident
   const float Ls0 = (float)(L[0] * kFixInv), Ls1 = (float)(L[1] * kFixInv), Ls2 = (float)(L[2] * kFixInv);
   const float rc2 = (float)(c.rc * c.rc);
-  const int4 ui = __ldg(base + li);
+  const int4 ui = valid ? __ldg(base + li) : make_int4(0, 0, 0, 0);
   const int xi = ui.x, yi = ui.y, zi = ui.z;
   // far bound: |d_x| below it keeps every site-pair component below L/2 - kImageTol
   float bnd0 = 0.f, bnd1 = 0.f, bnd2 = 0.f;
@@ -690,39 +815,39 @@ __device__ void tight_lists_f32(const DevPtrs& d, const RepConst& c, int li, con
     const float m = 2.f * (float)c.site_reach + kImageTol + 1e-3f;
     bnd0 = 0.5f * (float)L[0] - m; bnd1 = 0.5f * (float)L[1] - m; bnd2 = 0.5f * (float)L[2] - m;
   }
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << sub) - 1u;
   const int back = c.nbr_cap - 1;
   int nfar = 0, nnear = 0;
-  auto keep = [&](int j, float dx, float dy, float dz) {
-    if (dx * dx + dy * dy + dz * dz <= rc2) {
-      if (SIMG && (fabsf(dx) >= bnd0 || fabsf(dy) >= bnd1 || fabsf(dz) >= bnd2)) {
-        nt[(long long)(back - nnear) * T] = (uint16_t)j;
-        nnear++;
-      } else {
-        nt[(long long)nfar * T] = (uint16_t)j;
-        nfar++;
-      }
-    }
-  };
-  constexpr int B = 8;
-  int k = 0;
-  for (; k + B <= cnt; k += B) {
+  const int rounds = __reduce_max_sync(0xffffffffu, (cnt + kListLanes - 1) / kListLanes);
+  constexpr int B = 4;
+  for (int r0 = 0; r0 < rounds; r0 += B) {
     int j[B];
     int4 u[B];
 #pragma unroll
-    for (int m = 0; m < B; m++) j[m] = nb[(long long)(k + m) * T];
+    for (int m = 0; m < B; m++) {
+      const int k = (r0 + m) * kListLanes + sub;
+      j[m] = (k < cnt) ? (int)nb[(long long)k * T] : -1;
+    }
 #pragma unroll
-    for (int m = 0; m < B; m++) u[m] = __ldg(base + j[m]);
+    for (int m = 0; m < B; m++) u[m] = (j[m] >= 0) ? __ldg(base + j[m]) : ui;
 #pragma unroll
-    for (int m = 0; m < B; m++)
-      keep(j[m], (float)wrap_diff(xi, u[m].x) * Ls0, (float)wrap_diff(yi, u[m].y) * Ls1,
-           (float)wrap_diff(zi, u[m].z) * Ls2);
+    for (int m = 0; m < B; m++) {
+      const float dx = (float)wrap_diff(xi, u[m].x) * Ls0, dy = (float)wrap_diff(yi, u[m].y) * Ls1,
+                  dz = (float)wrap_diff(zi, u[m].z) * Ls2;
+      const bool in = j[m] >= 0 && dx * dx + dy * dy + dz * dz <= rc2;
+      const bool near = SIMG && in && (fabsf(dx) >= bnd0 || fabsf(dy) >= bnd1 || fabsf(dz) >= bnd2);
+      const unsigned gf = group_bits(__ballot_sync(0xffffffffu, in && !near), lane);
+      if (in && !near) nt[(long long)(nfar + __popc(gf & below)) * T] = (uint16_t)j[m];
+      nfar += __popc(gf);
+      if (SIMG) {
+        const unsigned gn = group_bits(__ballot_sync(0xffffffffu, near), lane);
+        if (near) nt[(long long)(back - nnear - __popc(gn & below)) * T] = (uint16_t)j[m];
+        nnear += __popc(gn);
+      }
+    }
   }
-  for (; k < cnt; k++) {
-    const int j = nb[(long long)k * T];
-    const int4 u = __ldg(base + j);
-    keep(j, (float)wrap_diff(xi, u.x) * Ls0, (float)wrap_diff(yi, u.y) * Ls1, (float)wrap_diff(zi, u.z) * Ls2);
-  }
-  d.nt_cnt[c.mol_off + li] = nfar | (nnear << 16);
+  if (valid && sub == 0) d.nt_cnt[c.mol_off + li] = nfar | (nnear << 16);
 }
 
 template <int S, int C0, bool SIMG>
@@ -1197,8 +1322,9 @@ __global__ void __launch_bounds__(128, 1) k_force_f64(DevPtrs d, const RepState*
 }
 
 // FP32 form, first launch after the replica head: skin-list rebuild when due,
-// pass 1.  Light on registers, so many warps hide the gathered loads of pass 1.
-__global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepState* __restrict__ X, int tile_size) {
+// pass 1; kListLanes x tile threads, the lanes of a molecule adjacent in a
+// warp.  Light on registers, so many warps hide the gathered loads.
+__global__ void __launch_bounds__(256, 4) k_force_lists(DevPtrs d, const RepState* __restrict__ X, int tile_size) {
   extern __shared__ uint32_t bm[];
   __shared__ double Ls[3];
   __shared__ int rb;
@@ -1209,16 +1335,27 @@ __global__ void __launch_bounds__(128, 6) k_force_lists(DevPtrs d, const RepStat
   if (threadIdx.x == 0) rb = d.cgrid[t.rep].rebuild;
   __syncthreads();
   const double L[3] = {Ls[0], Ls[1], Ls[2]};
-  const int i = threadIdx.x;
+  const int i = threadIdx.x / kListLanes, sub = threadIdx.x % kListLanes;
   const int li = t.start + i;
+  const bool valid = i < t.count;
   uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
-  if (rb) rebuild_tile<kF32>(d, c, t, tix, L, nb, tile_size, bm, d.bm_win);
-  if (i < t.count) {
-    uint16_t* nt = d.nbt + (nb - d.nbr);
-    const int cnt = d.nbr_cnt[c.mol_off + li];
-    if (site_image_needed(c, L)) tight_lists_f32<true>(d, c, li, L, nb, nt, cnt);
-    else tight_lists_f32<false>(d, c, li, L, nb, nt, cnt);
+  int cnt;
+  if (rb) {
+    cnt = build_lists_f32(d, c, t, L, nb, tile_size, bm, d.bm_win);
+    if (valid && sub == 0) {
+      const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+      d.ref_com[c.mol_off + li] = make_int4(w[0], w[1], w[2], 0);
+    }
+    if (threadIdx.x == 0)
+      for (int x = 0; x < 3; x++) d.Lbuild[3 * tix + x] = L[x];
+    __syncthreads();   // the group's list entries, written by all its lanes, are read below
+  } else {
+    cnt = valid ? d.nbr_cnt[c.mol_off + li] : 0;
   }
+  if (!valid) cnt = 0;
+  uint16_t* nt = d.nbt + (nb - d.nbr);
+  if (site_image_needed(c, L)) tight_lists_f32<true>(d, c, li, valid, sub, L, nb, nt, cnt, tile_size);
+  else tight_lists_f32<false>(d, c, li, valid, sub, L, nb, nt, cnt, tile_size);
 }
 
 // FP32 form, second launch of a step: pair forces, wall, A2M (box from X, which
@@ -1859,7 +1996,7 @@ void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int pre
   else k_replica_head<false><<<d.nrep_l, kRepThreads, 0, s>>>(d, Yin, Xout);
   const size_t bms = bitmap_smem_bytes(tile, d.bm_win);
   if (prec == kF32) {
-    k_force_lists<<<d.ntiles, tile, bms, s>>>(d, Xout, tile);
+    k_force_lists<<<d.ntiles, kListLanes * tile, bms, s>>>(d, Xout, tile);
     k_force_pairs<<<d.ntiles, kPairChunks * tile, force_smem_bytes(kPairChunks * tile), s>>>(d, Xout, tile);
   } else {
     k_force_f64<<<d.ntiles, tile, bms, s>>>(d, Xout, tile);
