@@ -328,9 +328,11 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
         # (the server admits them all within the budget used here)
         units_round = sum(jobs[k][0].spec.nmol * jobs[k][0].nreplica * jobs[k][0].spec.interval
                           for k in active)
+        changes0 = srv.stats()["batch_changes"]
         r0 = time.perf_counter()
         srv.step()
-        rounds.append(((time.perf_counter() - r0) * 1e3, units_round))
+        rounds.append(((time.perf_counter() - r0) * 1e3, units_round,
+                       srv.stats()["batch_changes"] != changes0))
         now = time.perf_counter() - t0
         for k in sorted(active):
             st = srv.poll(ids[k]).state
@@ -352,8 +354,21 @@ def run_stream(jobs, arrivals, budget, dev, one_at_a_time, seed0=1000):
             "max_graph_ms": stats["max_graph_ms"],
             # round time per million molecule-steps of its interval: the batch grows
             # and shrinks as jobs come and go, which alone spreads the round times
-            "p50_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u in rounds], 50)),
-            "p99_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u in rounds], 99))}
+            "p50_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u, _ in rounds], 50)),
+            "p99_round_ms_per_Mmolstep": float(np.percentile([r / (u * 1e-6) for r, u, _ in rounds], 99)),
+            # the same split by whether the round changed a batch (admission or exit)
+            "rounds_steady": round_stats([x for x in rounds if not x[2]]),
+            "rounds_with_batch_change": round_stats([x for x in rounds if x[2]])}
+
+
+def round_stats(rounds):
+    if not rounds:
+        return {"n": 0}
+    ms = [r for r, _, _ in rounds]
+    per = [r / (u * 1e-6) for r, u, _ in rounds]
+    return {"n": len(rounds), "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+            "p50_ms_per_Mmolstep": float(np.percentile(per, 50)),
+            "p99_ms_per_Mmolstep": float(np.percentile(per, 99))}
 
 
 def serving_sample(seed, njobs, warmup, budget_gib, dev, world):
@@ -875,6 +890,8 @@ def engine_arm(args, rank, world, local):
                    "max_graph_ms": sb["max_graph_ms"],
                    "p50_round_ms_per_Mmolstep": sb["p50_round_ms_per_Mmolstep"],
                    "p99_round_ms_per_Mmolstep": sb["p99_round_ms_per_Mmolstep"],
+                   "rounds_steady": sb["rounds_steady"],
+                   "rounds_with_batch_change": sb["rounds_with_batch_change"],
                    "interval_latency": "wall time of one server round: admission, any batch change, "
                                        "the interval's graph launch and the averages' read-back"}
 

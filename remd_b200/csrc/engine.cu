@@ -539,6 +539,11 @@ remd_status engine_get_exchange(remd_handle h, long long* steps, int* index) {
 
 size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
 
+void engine_prepare_wall(const remd_system_desc& s) {
+  std::string why;
+  if (s.confined > 0 && check_desc(s, why) == REMD_OK) wall_table_cached(s);
+}
+
 double engine_last_graph_ms(remd_handle h) { return h ? h->last_graph_ms : 0.0; }
 
 remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,

@@ -1,7 +1,8 @@
 // kernels.cuh -- the engine's CUDA kernels (sm_100a).
 //
 // One MD step of every replica of every ensemble is a short chain of launches
-// (a tile = `blockDim.x` consecutive molecules of one replica):
+// (a tile = 32 or 64 consecutive molecules of one replica, up to 128 in the
+// FP64 form):
 //
 //   k_integrate     [end of the previous step: D5 kick, D5/D6 scalars]
 //                   D6, D5, D4, D3 D2 D1 D2 D3 (src/integrator.cxx:646-673),
@@ -9,8 +10,8 @@
 //                   of mass + rotated site offsets) and the partial sums PsPv needs;
 //   k_replica_head  per replica: PsPv + D4 (scalar chain), the neighbour-list
 //                   decision and, when a rebuild is due, the cell lists;
-//   k_force_lists   per tile (FP32): the list rebuild from the cells when due,
-//                   then the per-step list of the pairs within rcut;
+//   k_force_lists   per tile (FP32, four lanes per molecule): the list rebuild
+//                   when due, then the per-step list of the pairs within rcut;
 //   k_force_pairs   per tile (FP32): the switched LJ + Coulomb pair loop, the
 //                   wall, and the site -> molecule torque (A2M);
 //   k_force_f64     per tile (FP64 form): rebuild, pair loop, wall, A2M.

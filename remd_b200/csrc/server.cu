@@ -26,6 +26,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -36,6 +37,7 @@
 namespace remd {
 remd_status engine_get_exchange(remd_handle h, long long* steps, int* index);
 size_t engine_bytes(remd_handle h);
+void engine_prepare_wall(const remd_system_desc& s);
 double engine_last_graph_ms(remd_handle h);
 remd_status engine_create_carry(remd_handle from, const remd_system_desc* systems, int nens,
                                 const int* reps_per_ens, const remd_replica_init* reps, const int* src_rep,
@@ -70,6 +72,7 @@ struct Job {
   int ens_in_batch = -1;           // ensemble of the current batch handle, -1 before admission
   int rep_in_batch = -1;           // its first replica there
   std::vector<double> avg;         // latest averages, nrep x 19
+  std::future<void> wall;          // its wall table, computed in the background from submission
   size_t bytes = 0;
   int nrep() const { return nt * np; }
 };
@@ -303,6 +306,10 @@ remd_status remd_job_submit(remd_server S, const remd_job_desc* jd, remd_job_id*
     j->index.push_back(k);
   }
   j->bytes = estimate_bytes(j->sys, j->nrep());
+  // a confined job's wall table (about a second of host time for a 65536-entry
+  // tube table on few cores) is computed while the job waits in the queue, so
+  // that admitting it does not stall the round that builds its batch
+  if (j->sys.confined > 0) j->wall = std::async(std::launch::async, engine_prepare_wall, j->sys);
   std::lock_guard<std::mutex> lk(S->mu);
   if (j->bytes > S->budget) {
     delete j;
@@ -482,6 +489,7 @@ remd_status remd_server_step(remd_server S, int* pending) {
     Job* j = S->queue.front();
     if (S->in_use + j->bytes > S->budget) break;
     S->queue.erase(S->queue.begin());
+    if (j->wall.valid()) j->wall.get();   // its wall table is in the engine's cache
     Batch* B = nullptr;
     for (Batch& b : S->batches)
       if (b.interval == j->sys.interval) B = &b;
