@@ -67,7 +67,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-serving", action="store_true",
                     help="config 4: skip the bounded serving sample (config 5's first --jobs jobs)")
     ap.add_argument("--cpu-steps", type=int, default=0, help="MD steps of the CPU sample (0: auto)")
-    ap.add_argument("--study", choices=["drift", "lists", "clusters"], default=None,
+    ap.add_argument("--study", choices=["drift", "lists", "clusters", "atomics"], default=None,
                     help="drift: NP Hamiltonian drift of the precision-study system (config 3), "
                          "FP32 form on every replica and FP64 vs FP32 on a subset")
     ap.add_argument("--drift-ps", type=float, default=100.0, help="drift study length (ps)")
@@ -653,6 +653,25 @@ def clusters_study(args, rank, world, local):
                       "summary": summary, "ensembles": out}), flush=True)
 
 
+def atomics_study(args, rank, world, local):
+    """Integer-add throughput (remd_measure_atomics) beside the pair work a
+    Newton's-third-law force step would add with it: config 4's unordered pairs
+    within rcut (seed 4, the bench's equilibrated state has 7.96 M) x 7 values
+    (force, space-frame torque and its scalar part) per pair."""
+    import ctypes
+
+    from remd_b200 import engine as E
+    rates = (ctypes.c_double * 4)()
+    E._check(E.lib().remd_measure_atomics(local, rates))
+    names = ["shared_u64", "shared_u32", "cluster_peer_u64", "global_u64"]
+    adds = 7.96e6 * 7
+    print(json.dumps({"study": "atomics", "unit": "G adds/s",
+                      "rates": {n: rates[k] for k, n in enumerate(names)},
+                      "adds_per_force_step": adds,
+                      "us_per_force_step_at_rate": {n: adds / (rates[k] * 1e9) * 1e6
+                                                    for k, n in enumerate(names)}}), flush=True)
+
+
 # ------------------------------------------------------------------ engine arm
 def profile_traffic():
     """DRAM bytes per force launch from the committed ncu summary, if present."""
@@ -945,6 +964,8 @@ def main():
             lists_study(args, rank, world, local)
         elif args.study == "clusters":
             clusters_study(args, rank, world, local)
+        elif args.study == "atomics":
+            atomics_study(args, rank, world, local)
         elif args.config == 5:
             serving_arm(args, rank, world, local)
         else:

@@ -192,6 +192,14 @@ remd_status remd_profile_steps(remd_handle h, int nsteps, double *ms_out);
  * kernel's roofline. */
 remd_status remd_measure_fp32_peak(int device, double *tflops);
 
+/* Integer-add throughput of this GPU in G adds/s, rates[0..3]: 64-bit into
+ * shared memory, 32-bit into shared memory, 64-bit into the shared memory of
+ * a peer block of a four-block cluster, 64-bit into global memory (L2).  Each
+ * of 4 blocks x 512 threads per SM adds to pseudo-random words of a 41 KB
+ * array (7 values x 736 molecules).  The rates at which a pair kernel that
+ * computes each pair once could add the partner's share in fixed point. */
+remd_status remd_measure_atomics(int device, double *rates);
+
 /* Per-replica health word of the last interval: 0 ok, else a remd_status. */
 remd_status remd_replica_status(remd_handle h, int rep, int *status);
 

@@ -1227,6 +1227,14 @@ remd_status remd_measure_fp32_peak(int device, double* tflops) {
   return REMD_OK;
 }
 
+remd_status remd_measure_atomics(int device, double* rates) {
+  if (!rates) return REMD_ERR_INVALID;
+  CK(cudaSetDevice(device));
+  const int s = measure_atomics(device, rates);
+  if (s != 0) { set_error("atomic throughput probe failed"); return (remd_status)s; }
+  return REMD_OK;
+}
+
 remd_status remd_replica_status(remd_handle h, int rep, int* status) {
   if (!h || !status || rep < 0 || rep >= h->nrep) return REMD_ERR_INVALID;
   CK(cudaMemcpy(status, h->d.status + rep, 4, cudaMemcpyDeviceToHost));

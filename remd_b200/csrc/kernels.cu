@@ -1,5 +1,6 @@
 // kernels.cu -- device code of the B200 REMD engine.  See kernels.cuh for the
 // step decomposition and engine_types.cuh for the data layout.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -9,6 +10,8 @@
 
 #include "integrator.cuh"
 #include "kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace remd {
 
@@ -1827,6 +1830,102 @@ int measure_fp32_fma(int device, double* ms, long long* flops) {
   *ms = best;
   *flops = (long long)blocks * threads * iters * 16LL * 8LL * 2LL;
   return 0;
+}
+
+// Throughput of integer adds into shared memory (64- and 32-bit), into a peer
+// block's shared memory (clusters of four) and into global memory (L2): the
+// rates at which a pair kernel that computes each pair once could add the
+// partner molecule's share of the forces.  Fixed-point sums do not depend on
+// the order of their terms, so such a kernel would stay deterministic.  Each
+// thread adds to pseudo-random words of a per-block array of kAtomWords words
+// (7 values x 736 molecules); every index is taken modulo that size.
+constexpr int kAtomWords = 7 * 736;
+constexpr int kAtomThreads = 512, kAtomBlocksPerSM = 4, kAtomIters = 4096;
+
+__device__ __forceinline__ unsigned atom_hash(unsigned x) {
+  x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+  return x;
+}
+
+template <int MODE>   // 0 shared u64, 1 shared u32, 2 u64 into cluster peers, 3 global u64
+__global__ void __launch_bounds__(kAtomThreads) k_atomic_rate(unsigned long long* gbuf, unsigned long long* out,
+                                                              int iters) {
+  extern __shared__ unsigned long long ash[];
+  for (int k = threadIdx.x; k < kAtomWords; k += blockDim.x) ash[k] = 0ull;
+  if (MODE == 2) cg::this_cluster().sync(); else __syncthreads();
+  unsigned long long* g = gbuf + (size_t)blockIdx.x * kAtomWords;
+  unsigned s = atom_hash(threadIdx.x * 7919u + blockIdx.x * 104729u);
+  for (int it = 0; it < iters; it++) {
+    s = atom_hash(s + (unsigned)it);
+    const int idx = (int)(s % (unsigned)kAtomWords);
+    if (MODE == 0) atomicAdd(&ash[idx], (unsigned long long)(s & 1023u));
+    if (MODE == 1) atomicAdd(reinterpret_cast<unsigned*>(ash) + idx, s & 1023u);
+    if (MODE == 2) atomicAdd(cg::this_cluster().map_shared_rank(ash, (int)((s >> 20) & 3u)) + idx,
+                             (unsigned long long)(s & 1023u));
+    if (MODE == 3) atomicAdd(g + idx, (unsigned long long)(s & 1023u));
+  }
+  // a cluster's blocks leave only when no peer adds into their memory any more
+  if (MODE == 2) cg::this_cluster().sync(); else __syncthreads();
+  unsigned long long t = 0ull;
+  for (int k = threadIdx.x; k < kAtomWords; k += blockDim.x) t += ash[k];
+  if (t == 0x5eedull) atomicAdd(out, t);   // keeps the adds live
+}
+
+int measure_atomics(int device, double* rates) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 6;
+  const int blocks = prop.multiProcessorCount * kAtomBlocksPerSM;   // 148 SMs: a multiple of 4
+  if (blocks % 4) return 6;
+  const size_t smem = kAtomWords * sizeof(unsigned long long);
+  unsigned long long *g = nullptr, *out = nullptr;
+  if (cudaMalloc(&g, (size_t)blocks * smem) != cudaSuccess) return 2;
+  if (cudaMalloc(&out, 8) != cudaSuccess) { cudaFree(g); return 2; }
+  cudaMemset(g, 0, (size_t)blocks * smem);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto launch = [&](int mode, int iters) {
+    if (mode == 2) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(blocks);
+      cfg.blockDim = dim3(kAtomThreads);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 4;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      cudaLaunchKernelEx(&cfg, k_atomic_rate<2>, g, out, iters);
+    } else if (mode == 0) {
+      k_atomic_rate<0><<<blocks, kAtomThreads, smem>>>(g, out, iters);
+    } else if (mode == 1) {
+      k_atomic_rate<1><<<blocks, kAtomThreads, smem>>>(g, out, iters);
+    } else {
+      k_atomic_rate<3><<<blocks, kAtomThreads, smem>>>(g, out, iters);
+    }
+  };
+  for (int mode = 0; mode < 4; mode++) {
+    launch(mode, 64);   // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+      cudaEventRecord(e0);
+      launch(mode, kAtomIters);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      best = fminf(best, t);
+    }
+    rates[mode] = (double)blocks * kAtomThreads * kAtomIters / (best * 1e-3) / 1e9;
+  }
+  const cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(g);
+  cudaFree(out);
+  return err == cudaSuccess ? 0 : 6;
 }
 
 // ------------------------------------------------------------------ caller-buffer variant

@@ -62,6 +62,7 @@ void launch_noalloc_load(const DevPtrs& d, const NoAllocSetup& setup, RepState* 
                          const double* q_aos, int tile, cudaStream_t s);
 void launch_noalloc_store(const DevPtrs& d, double* f_aos, double* n_aos, double* out, cudaStream_t s);
 int measure_fp32_fma(int device, double* ms, long long* flops);
+int measure_atomics(int device, double* rates);
 // Copies carried replicas from handle arrays `o` into `d` (serving batch changes):
 // molecule state (when `molecules`), RepState, pending condition, and per
 // carried ensemble the exchange index, counter and seed.

@@ -96,6 +96,7 @@ def lib():
         L.remd_stream.argtypes = [C.c_void_p]
         L.remd_profile_steps.argtypes = [C.c_void_p, C.c_int, _dp]
         L.remd_measure_fp32_peak.argtypes = [C.c_int, _dp]
+        L.remd_measure_atomics.argtypes = [C.c_int, _dp]
         L.remd_autotune.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp]
         L.remd_execute_steps_async.argtypes = [C.c_void_p, _dp, _dp]
         L.remd_get_averages.argtypes = [C.c_void_p, C.c_int, _dp]
