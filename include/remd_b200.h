@@ -82,7 +82,7 @@ typedef struct {
   int confined;             /* 0 bulk, 1 nanotube, 2 nano-slit                   */
   double dt_fs;
   double rcut, rswitch;     /* A */
-  int nfwall;
+  int nfwall;               /* wall table entries, 3 .. 16777216 (confined only)  */
   double wall_length;       /* A: tube radius or slit width                       */
   double sgm_wall, eps_wall, rho_wall;
   int interval;             /* MD steps per ExecuteSteps call                    */

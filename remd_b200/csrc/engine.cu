@@ -12,6 +12,7 @@
 #include <fstream>
 #include <iomanip>
 #include <map>
+#include <new>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -99,15 +100,18 @@ struct remd_engine_s {
 // once per entry (about a second of host time for 65536 entries), and a
 // serving batch is rebuilt whenever a job joins or leaves it; the tables of the
 // jobs still running come from here instead of being computed again.  The
-// cache keeps the most recent kWallCacheMax tables (1 MB each at 65536 entries).
+// cache keeps the most recent tables up to kWallCacheBytes in all (1 MB per
+// table at 65536 entries), and always the newest one.
 using WallKey = std::tuple<int, int, double, double, double, double>;
 static WallKey wall_key(const remd_system_desc& s) {
   return WallKey(s.confined, s.nfwall, s.wall_length, s.sgm_wall, s.eps_wall, s.rho_wall);
 }
-constexpr size_t kWallCacheMax = 64;
+constexpr int kMaxWallEntries = 1 << 24;             // 256 MB per table
+constexpr size_t kWallCacheBytes = size_t(256) << 20;
 static std::mutex g_wall_mu;
 static std::map<WallKey, std::shared_ptr<const std::vector<double>>> g_wall_cache;
 static std::deque<WallKey> g_wall_order;   // oldest first
+static size_t g_wall_bytes = 0;
 
 static std::shared_ptr<const std::vector<double>> wall_table_cached(const remd_system_desc& s) {
   const WallKey k = wall_key(s);
@@ -121,8 +125,11 @@ static std::shared_ptr<const std::vector<double>> wall_table_cached(const remd_s
   std::lock_guard<std::mutex> g(g_wall_mu);
   if (g_wall_cache.emplace(k, t).second) {
     g_wall_order.push_back(k);
-    if (g_wall_order.size() > kWallCacheMax) {
-      g_wall_cache.erase(g_wall_order.front());
+    g_wall_bytes += t->size() * sizeof(double);
+    while (g_wall_bytes > kWallCacheBytes && g_wall_order.size() > 1) {
+      auto it = g_wall_cache.find(g_wall_order.front());
+      g_wall_bytes -= it->second->size() * sizeof(double);
+      g_wall_cache.erase(it);
       g_wall_order.pop_front();
     }
   }
@@ -169,6 +176,7 @@ static remd_status check_desc(const remd_system_desc& s, std::string& why) {
   if (s.confined == 1 && (s.pconstant == 1 || s.pconstant == 3)) { why = "tube needs pconstant 0 or 2"; return REMD_ERR_INVALID; }
   if (s.confined == 2 && (s.pconstant == 1 || s.pconstant == 2)) { why = "slit needs pconstant 0 or 3"; return REMD_ERR_INVALID; }
   if (s.confined > 0 && (s.nfwall < 3 || s.wall_length <= 0.0)) { why = "confined system needs nfwall >= 3 and wall_length > 0"; return REMD_ERR_INVALID; }
+  if (s.confined > 0 && s.nfwall > kMaxWallEntries) { why = "nfwall must be <= 16777216"; return REMD_ERR_INVALID; }
   if (!(s.rcut > s.rswitch) || s.rswitch <= 0.0) { why = "need rcut > rswitch > 0"; return REMD_ERR_INVALID; }
   if (s.interval < 1) { why = "interval must be >= 1"; return REMD_ERR_INVALID; }
   if (!(s.dt_fs > 0.0)) { why = "dt must be > 0"; return REMD_ERR_INVALID; }
@@ -541,7 +549,11 @@ size_t engine_bytes(remd_handle h) { return h ? h->bytes : 0; }
 
 void engine_prepare_wall(const remd_system_desc& s) {
   std::string why;
-  if (s.confined > 0 && check_desc(s, why) == REMD_OK) wall_table_cached(s);
+  try {
+    if (s.confined > 0 && check_desc(s, why) == REMD_OK) wall_table_cached(s);
+  } catch (...) {
+    // out of host memory: the job's handle build computes the table again and reports it
+  }
 }
 
 double engine_last_graph_ms(remd_handle h) { return h ? h->last_graph_ms : 0.0; }
@@ -680,8 +692,14 @@ static remd_status create_impl(const remd_system_desc* systems, int nens, const 
       if (wall_key(systems[f]) == wall_key(s)) same = f;
     if (same >= 0) { wall_off[e] = wall_off[same]; continue; }
     wall_off[e] = (int)(h->wall_h.size() / 2);
-    const auto t = wall_table_cached(s);
-    h->wall_h.insert(h->wall_h.end(), t->begin(), t->end());
+    try {
+      const auto t = wall_table_cached(s);
+      h->wall_h.insert(h->wall_h.end(), t->begin(), t->end());
+    } catch (const std::bad_alloc&) {
+      set_error("system " + std::to_string(e) + ": no host memory for the wall table");
+      delete h;
+      return REMD_ERR_OOM;
+    }
   }
   // replicas
   int rep = 0, mol = 0;

@@ -8,6 +8,7 @@ Tolerances (relative L2 norms over all molecules unless stated):
   20-step trajectories (chaotic, errors grow ~e^(t/tau)): FP64 1e-8, FP32 see
   the per-quantity bounds in test_twenty_steps.
 """
+import copy
 import os
 
 import numpy as np
@@ -234,6 +235,29 @@ def test_velocity_scaling_modes_the_reference_does_not_integrate_are_rejected():
                              pconstant=pcon, tconstant=2)
         with pytest.raises(RuntimeError, match="tconstant 2"):
             E.REMDGPU([e], precision="fp32")
+
+
+def test_wall_tables_are_shared_cached_and_bounded():
+    """Ensembles with equal wall parameters share one table, a second handle
+    takes its table from the engine's cache (a tube table of 65536 entries is
+    about a second of host time), and neither changes a result; an nfwall
+    beyond the engine's bound is refused before any table is computed."""
+    a = S.small_ensemble("tip4p", 1, nmol=64, ntemp=1, npress=2, seed=57, interval=5, nfwall=65536)
+    b = S.small_ensemble("tip3p", 1, nmol=64, ntemp=1, npress=2, seed=58, interval=5, nfwall=65536)
+    alone = E.REMDGPU([a], precision="fp32")
+    alone.ExecuteSteps(a.T, a.P)
+    ref = [alone.ConvertVariablesToHost(r) for r in range(a.nreplica)]
+    alone.close()
+    both = E.REMDGPU([a, b], precision="fp32")
+    both.ExecuteSteps(np.concatenate([a.T, b.T]), np.concatenate([a.P, b.P]))
+    for r in range(a.nreplica):
+        g = both.ConvertVariablesToHost(r)
+        assert np.array_equal(g["r"], ref[r]["r"]) and np.array_equal(g["p"], ref[r]["p"])
+    both.close()
+    big = copy.deepcopy(a)
+    big.spec.nfwall = (1 << 24) + 1
+    with pytest.raises(RuntimeError, match="nfwall"):
+        E.REMDGPU([big], precision="fp32")
 
 
 def test_device_exchange_equals_host_exchange():
