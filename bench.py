@@ -249,11 +249,25 @@ def cpu_baseline(ens, nsteps, nthreads, variant="generic"):
             r.steps(nsteps)
         cores = 1
     dt = time.perf_counter() - t0
-    return {"value": molsteps / dt, "unit": METRIC, "cores": cores, "kind": kind,
+    return {"value": molsteps / dt, "unit": METRIC, "cores": cores, "kind": kind, "cpu": cpu_model(),
             "sample": f"all {len(refs)} replicas x {nsteps} MD steps "
                       f"({'oracle/_ref ' + variant + ' build' if kind == 'reference' else 'C oracle'},"
                       f" replica-parallel over {cores} threads; {dt:.1f} s timed, setup {setup:.1f} s)",
             "seconds": dt}
+
+
+def cpu_model():
+    """The host CPU's model name and its logical CPU count (the affinity mask
+    may allow fewer)."""
+    name = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                name = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical CPUs"
 
 
 def cpu_threads():
@@ -278,7 +292,7 @@ def reference_arm(args, rank, world):
             "ms_per_step": res["seconds"] * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_desc(args.config, ens, args.interval),
-            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "cpu", "sample")},
             "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "one step = one MD step of all replicas (bounded sample of the interval)"}
@@ -918,7 +932,7 @@ def engine_arm(args, rank, world, local):
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         nst = args.cpu_steps or 2
         cpu = cpu_baseline(ens, nst, cpu_threads())
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "cpu", "sample")}
         # config 1 (TIP4P nanotube) is the one workload the reference's tuned 4-site
         # CPU path is valid for: also time it as shipped (makefile.gnu flags, FP32
         # forces, replicas one after another) and as the tuned FP64 build
