@@ -184,6 +184,29 @@ def test_batch_equals_alone_bitwise():
             k += 1
 
 
+def test_dependent_launch_and_plain_launch_agree_bitwise():
+    """A step whose tile grid is no larger than the SM count is launched with
+    programmatic stream serialisation, a larger one plainly.  A small ensemble
+    alone (dependent launches) and the same ensemble inside a batch of more than
+    148 tiles per interval-graph chain (plain launches) give the same bits."""
+    small = S.small_ensemble("tip4p", 0, nmol=70, ntemp=2, npress=1, seed=34, interval=10)
+    filler = S.make_ensemble("filler", "tip3p", 0, 512, 0.0, 9.0, 8.0, 16, 4, 250, 350, 0.1e6, 0.1e6, 35,
+                             interval=10)
+    alone = E.REMDGPU([small], precision="fp32")
+    alone.set_tuning(32, 1.0)
+    alone.ExecuteSteps(small.T, small.P)
+    both = E.REMDGPU([small, filler], precision="fp32")
+    both.set_tuning(32, 1.0)
+    assert filler.nreplica * 16 // 4 > 148   # 512 molecules = 16 tiles of 32, over four chains
+    both.ExecuteSteps(np.concatenate([small.T, filler.T]), np.concatenate([small.P, filler.P]))
+    for r in range(small.nreplica):
+        assert np.array_equal(alone.GetAverages(r), both.GetAverages(r))
+        a, b = alone.ConvertVariablesToHost(r), both.ConvertVariablesToHost(r)
+        assert np.array_equal(a["r"], b["r"]) and np.array_equal(a["p"], b["p"])
+    alone.close()
+    both.close()
+
+
 def test_velocity_scaling_in_a_mixed_batch():
     """tconstant 2: Molecules::ExecuteSteps rescales the velocities before every
     step (src/integrator.cxx:713-723).  In a batch with Nose-Poincare replicas the
