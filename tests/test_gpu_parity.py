@@ -3,8 +3,8 @@
 Tolerances (relative L2 norms over all molecules unless stated):
   FP64 engine: forces/torques 1e-10, energies 1e-11 -- same arithmetic as the
                oracle, different summation order;
-  FP32 engine: forces and torques 1e-5, potential energy 1e-6 (the north-star
-               accuracy gate), virial 1e-5;
+  FP32 engine: forces and torques 1e-5, potential energy 1e-6 (the engine's
+               FP32 accuracy gate), virial 1e-5;
   20-step trajectories (chaotic, errors grow ~e^(t/tau)): FP64 1e-8, FP32 see
   the per-quantity bounds in test_twenty_steps.
 """
@@ -425,7 +425,7 @@ def test_long_fp64_trajectory_config4_ensembles(idx):
 
 @pytest.mark.parametrize("idx", range(8))
 def test_fp32_accuracy_liquid(idx):
-    """The north-star accuracy gate on the benchmark's own (liquid-density)
+    """The FP32 accuracy gate on the benchmark's own (liquid-density)
     ensembles: force and torque RMS error <= 1e-5 relative, potential energy
     within 1e-6 relative of the FP64 oracle, one replica per ensemble."""
     e = S.config4(seed=4)[idx]
