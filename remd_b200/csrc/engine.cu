@@ -677,7 +677,7 @@ static remd_status create_impl(const remd_system_desc* systems, int nens, const 
   auto* h = new remd_engine_s;
   h->device = device;
   h->prec = (prec == REMD_PREC_FP64) ? kF64 : kF32;
-  h->tile = (h->prec == kF32) ? 32 : 128;   // measured best on config 4; remd_set_tuning / remd_autotune change it
+  h->tile = (h->prec == kF32) ? 32 : 128;   // measured best on a 256-replica mixed batch; remd_set_tuning / remd_autotune change it
   h->nens = nens;
   h->interval = systems[0].interval;
   h->sys.assign(systems, systems + nens);

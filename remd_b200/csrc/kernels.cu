@@ -2090,9 +2090,10 @@ static int sm_count() {
 // with programmatic stream serialisation.  That pays where a step's tile grid
 // is smaller than the GPU (one block per SM or fewer): the launches are
 // latency-bound and the early-scheduled blocks wait on otherwise idle SMs
-// (config 1: 55 -> 58.5 M mol-steps/s).  Where the grid fills the GPU, the
-// waiting blocks hold slots that the other chains of the interval graph would
-// use (config 4: 288 -> 253 M with it), so those launches are plain.
+// (16 replicas of 128 TIP4P molecules: 55 -> 58.5 M mol-steps/s).  Where the
+// grid fills the GPU, the waiting blocks hold slots that the other chains of
+// the interval graph would use (256 replicas, 111 432 molecules: 288 -> 253 M
+// with it), so those launches are plain.
 template <typename... KArgs, typename... Args>
 static void launch_step_kernel(bool pdl, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem,
                                cudaStream_t s, Args... args) {
