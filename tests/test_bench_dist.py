@@ -65,3 +65,23 @@ def test_replicas_only_aggregation_two_ranks():
     assert out[0][4] != out[1][4]
     # the reference arm prints only on rank 0
     assert out[1][5] == ""
+
+
+def test_round_stats_split_and_normalisation():
+    """Serving round statistics: raw p50/p99 milliseconds and milliseconds per
+    million molecule-steps of the round's interval, per class of round."""
+    import bench
+    rounds = [(10.0, 2e6, False), (20.0, 2e6, False), (40.0, 1e6, True)]
+    steady = bench.round_stats([r for r in rounds if not r[2]])
+    changed = bench.round_stats([r for r in rounds if r[2]])
+    assert steady["n"] == 2 and changed["n"] == 1
+    assert steady["p50_ms"] == pytest.approx(15.0)
+    assert steady["p50_ms_per_Mmolstep"] == pytest.approx(7.5)
+    assert changed["p99_ms_per_Mmolstep"] == pytest.approx(40.0)
+    assert bench.round_stats([]) == {"n": 0}
+
+
+def test_cpu_model_names_the_host():
+    import bench
+    s = bench.cpu_model()
+    assert s.endswith("logical CPUs") and str(os.cpu_count()) in s
