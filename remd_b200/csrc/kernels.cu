@@ -425,8 +425,10 @@ __global__ void __launch_bounds__(kRepThreads) k_replica_head(DevPtrs d, const R
   }
 }
 
-// Neighbour-list rebuild for the molecules of this tile.  The list of molecule
-// i holds, in ascending j, every j that passes the list test (below):
+// Neighbour-list rebuild for the molecules of this tile, one lane per molecule
+// (build_lists, the FP64 form; the FP32 form's build_lists_f32 below gives the
+// same lists with four lanes per molecule).  The list of molecule i holds, in
+// ascending j, every j that passes the list test (below):
 //  * a replica not cut into cells (CellGrid 1 x 1 x 1): every molecule of the
 //    replica is tested, 128 candidates at a time from shared memory (all lanes
 //    read the same candidate: a broadcast), which emits them in ascending j;
@@ -464,7 +466,6 @@ __device__ __forceinline__ bool list_test(const int4 me, const int4 cj, float ls
   return dx * dx + dy * dy + dz * dz < rl2;
 }
 
-template <int PREC>
 __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, const double* L,
                             uint16_t* nb, int tile_size, uint32_t* bm, int win) {
   __shared__ double4 cand[128];
@@ -473,24 +474,15 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
   const int li = t.start + i;
   const double rl = c.rc + c.skin;
   const double rl2 = rl * rl;
-  const float lsc0 = (float)(L[0] * (1.0 / 65536.0)), lsc1 = (float)(L[1] * (1.0 / 65536.0)),
-              lsc2 = (float)(L[2] * (1.0 / 65536.0));
-  float rl2f = 0.f;
-  if (PREC == kF32) {
-    const double rw = list_test_radius(c, L);
-    rl2f = (float)(rw * rw);
-  }
-  const int4* com = d.com + c.mol_off;
+  const int4* com = d.com + c.mol_off;   // cell coordinates of the centres
   const double* pk = reinterpret_cast<const double*>(d.pack) + c.pack_off;
   int4 me = make_int4(0, 0, 0, 0);
   double rx = 0, ry = 0, rz = 0;
   if (valid) {
     me = com[li];
-    if (PREC == kF64) {
-      rx = pk[(long long)li * c.pack_stride];
-      ry = pk[(long long)li * c.pack_stride + 1];
-      rz = pk[(long long)li * c.pack_stride + 2];
-    }
+    rx = pk[(long long)li * c.pack_stride];
+    ry = pk[(long long)li * c.pack_stride + 1];
+    rz = pk[(long long)li * c.pack_stride + 2];
   }
   const CellGrid g = d.cgrid[t.rep];
   int cnt = 0;
@@ -499,20 +491,16 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
     for (int base = 0; base < c.nmol; base += 128) {
       __syncthreads();
       for (int k = threadIdx.x; k < 128 && base + k < c.nmol; k += blockDim.x) {
-        if (PREC == kF32) {
-          reinterpret_cast<int4*>(&cand[k])[0] = com[base + k];
-        } else {
-          const double* w = pk + (long long)(base + k) * c.pack_stride;
-          cand[k] = make_double4(w[0], w[1], w[2], 0);
-        }
+        const double* w = pk + (long long)(base + k) * c.pack_stride;
+        cand[k] = make_double4(w[0], w[1], w[2], 0);
       }
       __syncthreads();
       if (valid) {
         const int nk = min(128, c.nmol - base);
         for (int k = 0; k < nk; k++) {
           const int j = base + k;
-          const bool in = list_test<PREC>(me, reinterpret_cast<const int4*>(&cand[k])[0], lsc0, lsc1, lsc2,
-                                          rl2f, rx, ry, rz, reinterpret_cast<const double*>(&cand[k]), L, rl2);
+          const bool in = list_test<kF64>(me, make_int4(0, 0, 0, 0), 0.f, 0.f, 0.f, 0.f, rx, ry, rz,
+                                          reinterpret_cast<const double*>(&cand[k]), L, rl2);
           if (j != li && in) {
             if (cnt < c.nbr_cap) nb[(long long)cnt * tile_size] = (uint16_t)j;
             cnt++;
@@ -549,8 +537,8 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
               const int4 cj = cm[k];
               const int j = cj.w;
               if (j < jlo || j >= jhi || j == li) continue;
-              if (list_test<PREC>(me, cj, lsc0, lsc1, lsc2, rl2f, rx, ry, rz, pk + (long long)j * c.pack_stride,
-                                  L, rl2))
+              if (list_test<kF64>(me, cj, 0.f, 0.f, 0.f, 0.f, rx, ry, rz, pk + (long long)j * c.pack_stride, L,
+                                  rl2))
                 row[(j - jlo) >> 5] |= 1u << (j & 31);
             }
           }
@@ -579,7 +567,8 @@ __device__ void build_lists(const DevPtrs& d, const RepConst& c, const Tile& t, 
 
 // FP32 skin-list build for the list kernel, kListLanes lanes per molecule
 // (molecule slot threadIdx.x / kListLanes, lane sub = threadIdx.x % kListLanes).
-// The lists are those of build_lists<kF32>, entry for entry:
+// The lists are entry for entry those that build_lists gives with one lane per
+// molecule (the FP64 form still builds its lists that way):
 //  * all-molecule scan: lane sub tests candidates sub, sub + 4, ... of each
 //    128-molecule chunk staged in shared memory, and a ballot places the kept
 //    ones in ascending j;
@@ -1202,23 +1191,16 @@ __device__ inline void zero_acc(IAcc& a) {
   a.npair = 0;
 }
 
-// Skin-list rebuild of tile t when due, with the build's reference centres and box.
-template <int PREC>
+// FP64 form: skin-list rebuild of tile t when due, with the build's reference
+// centres and box.
 __device__ void rebuild_tile(const DevPtrs& d, const RepConst& c, const Tile& t, int tix, const double* L,
                              uint16_t* nb, int tile_size, uint32_t* bm, int win) {
   const int i = threadIdx.x;
   const int li = t.start + i;
-  build_lists<PREC>(d, c, t, L, nb, tile_size, bm, win);
+  build_lists(d, c, t, L, nb, tile_size, bm, win);
   if (i < t.count) {
-    int4 rc4;
-    if (PREC == kF32) {
-      const int* w = reinterpret_cast<const int*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-      rc4 = make_int4(w[0], w[1], w[2], 0);
-    } else {
-      const double* wd = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
-      rc4 = make_int4(fix_coord(wd[0]), fix_coord(wd[1]), fix_coord(wd[2]), 0);
-    }
-    d.ref_com[c.mol_off + li] = rc4;
+    const double* wd = reinterpret_cast<const double*>(d.pack) + c.pack_off + (long long)li * c.pack_stride;
+    d.ref_com[c.mol_off + li] = make_int4(fix_coord(wd[0]), fix_coord(wd[1]), fix_coord(wd[2]), 0);
   }
   if (i == 0)
     for (int x = 0; x < 3; x++) d.Lbuild[3 * tix + x] = L[x];
@@ -1237,7 +1219,7 @@ __device__ void force_tile_f64(const DevPtrs& d, const RepConst& c, const Tile& 
   const int li = t.start + i;
   const int g = c.mol_off + li;
   uint16_t* nb = d.nbr + c.nbr_off + (long long)(tix - c.tile_off) * c.nbr_cap * tile_size + i;
-  if (rebuild) rebuild_tile<kF64>(d, c, t, tix, L, nb, tile_size, bm, win);
+  if (rebuild) rebuild_tile(d, c, t, tix, L, nb, tile_size, bm, win);
   IAcc a;
   zero_acc(a);
   double wall_e = 0.0;

@@ -306,15 +306,21 @@ remd_status remd_job_submit(remd_server S, const remd_job_desc* jd, remd_job_id*
     j->index.push_back(k);
   }
   j->bytes = estimate_bytes(j->sys, j->nrep());
-  // a confined job's wall table (about a second of host time for a 65536-entry
-  // tube table on few cores) is computed while the job waits in the queue, so
-  // that admitting it does not stall the round that builds its batch
-  if (j->sys.confined > 0) j->wall = std::async(std::launch::async, engine_prepare_wall, j->sys);
   std::lock_guard<std::mutex> lk(S->mu);
   if (j->bytes > S->budget) {
     delete j;
     set_error("remd_job_submit: the job alone exceeds the HBM budget");
     return REMD_ERR_OOM;
+  }
+  // a confined job's wall table (about a second of host time for a 65536-entry
+  // tube table on few cores) is computed while the job waits in the queue, so
+  // that admitting it does not stall the round that builds its batch; without a
+  // thread for it, the batch build computes it
+  if (j->sys.confined > 0) {
+    try {
+      j->wall = std::async(std::launch::async, engine_prepare_wall, j->sys);
+    } catch (...) {
+    }
   }
   j->id = S->next_id++;
   j->t_submit = now_s() - S->t0;
