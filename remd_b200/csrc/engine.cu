@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <fstream>
@@ -691,6 +692,11 @@ static remd_status create_impl(const remd_system_desc* systems, int nens, const 
     for (int f = 0; f < e && same < 0; f++)
       if (wall_key(systems[f]) == wall_key(s)) same = f;
     if (same >= 0) { wall_off[e] = wall_off[same]; continue; }
+    if (h->wall_h.size() / 2 + (size_t)s.nfwall > (size_t)INT32_MAX) {
+      set_error("system " + std::to_string(e) + ": the handle's wall tables exceed 2^31 entries");
+      delete h;
+      return REMD_ERR_INVALID;
+    }
     wall_off[e] = (int)(h->wall_h.size() / 2);
     try {
       const auto t = wall_table_cached(s);
