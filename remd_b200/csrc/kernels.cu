@@ -702,10 +702,10 @@ struct IAcc {
 // (k_force_pairs).  Pass 1 runs in its own light kernel, whose occupancy hides
 // the latency of its gathered loads; pass 2 is register-heavy.
 // Pair math in FP32 (rsqrt on the SFU plus one Newton step); partial sums in
-// FP32 over 16 pairs, then FP64 accumulation into this thread's slots of `acc`
+// FP32 over 32 pairs, then FP64 accumulation into this thread's slots of `acc`
 // (shared memory, field f at acc[f * blockDim.x + threadIdx.x]: 3S site-force
 // components, 3 switching-correction, 3 virial, LJ, Coulomb).  The pairs within
-// rcut, their far/near class and order, and their grouping by 16 depend only
+// rcut, their far/near class and order, and their grouping by 32 depend only
 // on the positions, not on when the skin list was built.  The next
 // neighbour's index is read one pair ahead of its use.
 // SIMG: apply the minimum image to every site pair as the reference does
@@ -908,7 +908,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const F32Cons
     acc[(3 * S + 7) * T + tid] += (double)fcl;
   };
   zero();
-  int done = 0;                       // pairs accumulated (partial sums close every 16)
+  int done = 0;                       // pairs accumulated (partial sums close every 32)
   int ndef = 0, def0 = 0, def1 = 0;   // deferred site pairs (near pass only)
 
   // pass 2: `n` pairs of the list starting at column slot `pos0`, stepping `dir`;
@@ -1004,7 +1004,7 @@ __device__ void pair_loop_f32(const DevPtrs& d, const RepConst& c, const F32Cons
       fv[2] += fmaf(fpz, sw, cz) * dz;
       flj += sw * elj;
       fcl += sw * ecl;
-      if ((++done & 15) == 0) { flush(); zero(); }
+      if ((++done & 31) == 0) { flush(); zero(); }
     }
   };
   // positions [p0, p1) of the sequence far pairs (rows 0..) then near pairs (rows back, back-1, ..)
