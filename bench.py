@@ -559,8 +559,8 @@ def drift_study(args, rank, world, local):
 
 # ------------------------------------------------------------------ force step per system (list builds)
 def lists_study(args, rank, world, local):
-    """Force-step time (CUDA events over 50 MD steps, list rebuilds included:
-    remd_profile_steps) at fixed tile 32 and several skins, for the config-4
+    """Force-step time per launch (CUDA events over 50 MD steps, list rebuilds
+    included: remd_profile_split) at fixed tile 32 and several skins, for the config-4
     batch and for the largest systems of the serving stream (N = 4096: a 50 A
     TIP5P bulk box, a 1.4 um TIP4P nanotube, a 115 A TIP3P slit; 8 replicas
     each), with a hash of the positions and momenta after one more interval
@@ -580,16 +580,17 @@ def lists_study(args, rank, world, local):
         eng = E.REMDGPU(ens, precision="fp32", device=local, interval=10)
         eng.set_tuning(32, skin)
         eng.execute_nsteps(20)
-        prof = (ctypes.c_double * 2)()
-        E._check(E.lib().remd_profile_steps(eng.h, nsteps, prof))
+        prof = (ctypes.c_double * 5)()
+        E._check(E.lib().remd_profile_split(eng.h, nsteps, prof))
         eng.ExecuteSteps(np.concatenate([e.T for e in ens]), np.concatenate([e.P for e in ens]))
         h = hashlib.sha1()
         for r in range(min(eng.nrep, 8)):
             g = eng.ConvertVariablesToHost(r)
             h.update(g["r"].tobytes())
             h.update(g["p"].tobytes())
-        out[name] = {"force_ms": prof[1], "integrate_ms": prof[0], "skin": skin, "tile": 32,
-                     "trajectory_sha1": h.hexdigest()}
+        out[name] = {"force_ms": prof[1] + prof[2] + prof[3], "integrate_ms": prof[0], "head_ms": prof[1],
+                     "lists_ms": prof[2], "pairs_ms": prof[3], "rebuilt_replicas_per_step": prof[4],
+                     "skin": skin, "tile": 32, "trajectory_sha1": h.hexdigest()}
         eng.close()
 
     c4 = S.config4(seed=4)

@@ -187,6 +187,13 @@ void *remd_stream(remd_handle h);
  * bookkeeping (use on a scratch handle). */
 remd_status remd_profile_steps(remd_handle h, int nsteps, double *ms_out);
 
+/* remd_profile_steps with the force step split per launch: ms_out[0..3] the
+ * mean time per MD step of the integrate kernel, the replica head, the list
+ * kernel and the pair kernel (FP64 form: [2] = 0, [3] its one force kernel);
+ * ms_out[4] the mean number of replicas whose neighbour lists were rebuilt per
+ * step.  One launch chain, CUDA events between the launches. */
+remd_status remd_profile_split(remd_handle h, int nsteps, double *ms_out);
+
 /* FP32 FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) from a register-
  * resident FMA-chain kernel over every SM; the denominator of the force
  * kernel's roofline. */

@@ -1240,6 +1240,35 @@ remd_status remd_profile_steps(remd_handle h, int nsteps, double* ms_out) {
   return sync_and_check(h);
 }
 
+remd_status remd_profile_split(remd_handle h, int nsteps, double* ms_out) {
+  if (!h || nsteps < 1 || !ms_out) return REMD_ERR_INVALID;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double t[4] = {0, 0, 0, 0}, rebuilt = 0.0;
+  std::vector<CellGrid> g(h->nrep);
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaEventRecord(ev[0], h->stream));
+    launch_step_integrate(h, s);
+    CK(cudaEventRecord(ev[1], h->stream));
+    launch_force_timed(h->d, h->Y, h->X, h->prec, h->tile, h->stream, ev[2], ev[3]);
+    CK(cudaEventRecord(ev[4], h->stream));
+    CK(cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; k++) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      t[k] += ms;
+    }
+    CK(cudaMemcpy(g.data(), h->d.cgrid, h->nrep * sizeof(CellGrid), cudaMemcpyDeviceToHost));
+    for (const CellGrid& x : g) rebuilt += x.rebuild ? 1.0 : 0.0;
+  }
+  launch_replica_end(h->d, h->X, h->stream);
+  for (auto& e : ev) cudaEventDestroy(e);
+  h->steps_done += nsteps;
+  for (int k = 0; k < 4; k++) ms_out[k] = t[k] / nsteps;
+  ms_out[4] = rebuilt / nsteps;
+  return sync_and_check(h);
+}
+
 remd_status remd_measure_fp32_peak(int device, double* tflops) {
   if (!tflops) return REMD_ERR_INVALID;
   CK(cudaSetDevice(device));

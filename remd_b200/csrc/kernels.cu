@@ -2112,20 +2112,35 @@ cudaError_t force_kernel_setup() {
   return cudaFuncSetAttribute(k_force_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, bms);
 }
 
-void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
-                  int tile, cudaStream_t s) {
+// The force launches of one step; e_head / e_lists (may be null) are recorded
+// after the head and after the list kernel (profiling: remd_profile_split).
+static void launch_force_impl(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
+                              int tile, cudaStream_t s, cudaEvent_t e_head, cudaEvent_t e_lists) {
   const RepState* Xc = Xout;
   const bool pdl = d.ntiles <= sm_count();   // the step's tile grid (see launch_step_kernel)
   if (force_only) launch_step_kernel(pdl, k_replica_head<true>, d.nrep_l, kRepThreads, 0, s, d, Yin, Xout);
   else launch_step_kernel(pdl, k_replica_head<false>, d.nrep_l, kRepThreads, 0, s, d, Yin, Xout);
+  if (e_head) cudaEventRecord(e_head, s);
   const size_t bms = bitmap_smem_bytes(tile, d.bm_win);
   if (prec == kF32) {
     launch_step_kernel(pdl, k_force_lists, d.ntiles, kListLanes * tile, bms, s, d, Xc, tile);
+    if (e_lists) cudaEventRecord(e_lists, s);
     launch_step_kernel(pdl, k_force_pairs, d.ntiles, kPairChunks * tile, force_smem_bytes(kPairChunks * tile), s,
                        d, Xc, tile);
   } else {
+    if (e_lists) cudaEventRecord(e_lists, s);
     launch_step_kernel(pdl, k_force_f64, d.ntiles, tile, bms, s, d, Xc, tile);
   }
+}
+
+void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
+                  int tile, cudaStream_t s) {
+  launch_force_impl(d, Yin, Xout, prec, force_only, tile, s, nullptr, nullptr);
+}
+
+void launch_force_timed(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, int tile, cudaStream_t s,
+                        cudaEvent_t e_head, cudaEvent_t e_lists) {
+  launch_force_impl(d, Yin, Xout, prec, false, tile, s, e_head, e_lists);
 }
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s) {
   k_replica_start<<<d.nrep, kRepThreads, 0, s>>>(d, X);

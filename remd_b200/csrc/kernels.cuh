@@ -38,6 +38,10 @@ cudaError_t force_kernel_setup();
 int bitmap_window(int max_nmol);
 void launch_force(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, bool force_only,
                   int tile, cudaStream_t s);
+// launch_force(..., force_only = false, ...) with events recorded after the
+// replica head and after the list kernel (FP64 form: before its one kernel).
+void launch_force_timed(const DevPtrs& d, const RepState* Yin, RepState* Xout, int prec, int tile, cudaStream_t s,
+                        cudaEvent_t e_head, cudaEvent_t e_lists);
 void launch_replica_start(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_end(const DevPtrs& d, RepState* X, cudaStream_t s);
 void launch_replica_props(const DevPtrs& d, RepState* X, cudaStream_t s);

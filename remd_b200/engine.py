@@ -95,6 +95,7 @@ def lib():
         L.remd_stream.restype = C.c_void_p
         L.remd_stream.argtypes = [C.c_void_p]
         L.remd_profile_steps.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.remd_profile_split.argtypes = [C.c_void_p, C.c_int, _dp]
         L.remd_measure_fp32_peak.argtypes = [C.c_int, _dp]
         L.remd_measure_atomics.argtypes = [C.c_int, _dp]
         L.remd_autotune.argtypes = [C.c_void_p, C.c_int, _ip, _dp, _dp]
